@@ -1,0 +1,119 @@
+/*
+ * paragram_b200.h -- C ABI of the B200 diagram builder (libparagram_b200.so).
+ *
+ * Drop-in boundary for the reference's pybind entry points
+ *   laguerre::build_voronoi_ultra            (paragram/csrc/laguerre/laguerre.h:24-29,
+ *                                             bound at paragram/csrc/ext.cpp:21-29)
+ *   laguerre::build_laguerre_voronoi_ultra   (paragram/csrc/laguerre/laguerre.h:13-20,
+ *                                             bound at paragram/csrc/ext.cpp:10-19)
+ * which take CUDA tensors and return (adjacency, offsets, status). A C ABI
+ * cannot return tensors whose size is data dependent, so one reference call
+ * is split into plain-pointer steps:
+ *
+ *   pg_workspace_size(N, &bytes)          -> caller allocates `bytes` of device memory
+ *   pg_build(..., offsets, status, &E)    -> fills offsets [N+1] and status [N],
+ *                                            returns the adjacency length E
+ *                                            (the reference's cudaMemcpy of the total,
+ *                                            voronoi_ultra.cu:352-354)
+ *   pg_emit_adjacency(..., adjacency)     -> caller allocates E int32, this fills it
+ *
+ * All pointers except `options` are device pointers. Every call is ordered on
+ * `stream` (a cudaStream_t, NULL = legacy default stream); pg_build
+ * synchronises the stream once to read E back, like the reference.
+ * Outputs match the reference's Diagram: int32 CSR adjacency (rows sorted),
+ * int32 offsets of shape (N+1,), int32 per-point status
+ * (0 success, 1 plane_overflow, 2 vertex_overflow, 3 empty_cell,
+ * 4 security_radius_not_reached, 5 inconsistent_boundary;
+ * faster_convex_cell.cuh:99-108).
+ *
+ * Return codes: 0 on success, negative on error; pg_last_error() describes the
+ * last error of the calling thread. PG_ERR_INVALID corresponds to the
+ * reference's argument ASSERTs (std::runtime_error, voronoi_ultra.cu:20-24).
+ */
+#ifndef PARAGRAM_B200_H
+#define PARAGRAM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PG_OK 0
+#define PG_ERR_INVALID (-1)   /* bad argument (reference: ASSERT -> std::runtime_error) */
+#define PG_ERR_CUDA (-2)      /* CUDA runtime error (reference: cuda_check, cuda_helpers.h:79-102) */
+#define PG_ERR_INTERNAL (-3)  /* internal capacity exceeded */
+
+/* Options of one build. Mirrors the keyword arguments of the reference
+ * (paragram/_api.py:65-123; defaults at paragram/csrc/ext.cpp:14-19). */
+typedef struct pg_options
+{
+    int32_t knn;        /* reference: kNN(knn) warm start (voronoi_ultra.cu:205-227). Here knn > 0
+                           enables the curve-order warm start (32 Morton neighbours); 0 disables it.
+                           Results do not depend on it. Ignored when initial guesses are given
+                           (the reference sets knn = 0 then, voronoi_ultra.cu:157-169). */
+    int32_t leaf_size;  /* reference: BVH leaf threshold, -1 = default (voronoi_ultra.cu:175-177).
+                           Here <= 0 selects 16; at most 32. Results do not depend on it. */
+    int32_t debug;      /* reference: print phase timings (voronoi_ultra.cu:196-219). Bit 0 prints them,
+                           bit 1 only records them for pg_last_profile. */
+    int32_t num_chunks; /* reference: PARAGRAM_NUM_CHUNKS / PARAGRAM_MEM_FRAC chunk plan
+                           (chunking.h:16-56). 0 = read the environment; > 0 = split the cell
+                           pass into this many launches. Results do not depend on it. */
+} pg_options;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int pg_version(void);
+
+/* Message of the last error returned on this thread ("" if none). */
+const char *pg_last_error(void);
+
+/* Device workspace needed for num_points points (any weights / options).
+ * Replaces the reference's internal torch / cudaMalloc allocations
+ * (voronoi_ultra.cu:186, 207, 230-232, 267-268, 319-324; pwr_bvh.cu:228-269). */
+int pg_workspace_size(int64_t num_points, size_t *bytes);
+
+/* Build the diagram. Replaces build_voronoi_ultra (weights == NULL) and
+ * build_laguerre_voronoi_ultra (weights != NULL), laguerre.h:13-29.
+ *   points      float32 [num_points * 3], xyz interleaved (contiguous (N, 3) tensor)
+ *   weights     float32 [num_points] or NULL
+ *   initial_guesses / initial_guesses_offsets
+ *               int32 CSR of candidate neighbours per point (original ids), or both NULL
+ *               (reference: voronoi_ultra.cu:69-85). Results do not depend on them.
+ *   options     host pointer or NULL (defaults: knn 8, leaf_size -1, debug 0, num_chunks 0)
+ *   workspace   device buffer of at least pg_workspace_size() bytes, 256-byte aligned;
+ *               it must stay alive until pg_emit_adjacency returns
+ *   offsets     int32 [num_points + 1]  (output)
+ *   status      int32 [num_points]      (output)
+ *   num_edges   host int64              (output) = offsets[num_points]
+ */
+int pg_build(int64_t num_points, const float *points, const float *weights, const int32_t *initial_guesses,
+             const int32_t *initial_guesses_offsets, const pg_options *options, void *workspace,
+             size_t workspace_bytes, int32_t *offsets, int32_t *status, int64_t *num_edges, void *stream);
+
+/* Write the adjacency (int32 [num_edges]) of the last pg_build on this
+ * workspace. Replaces populate_symmetric_adjacency (adjacency.cuh:120-159). */
+int pg_emit_adjacency(int64_t num_points, const void *workspace, const int32_t *offsets, int32_t *adjacency,
+                      void *stream);
+
+/* Counters of the last pg_build on this workspace (synchronises the stream):
+ * out[0] FP32 side tests, out[1] tests escalated to FP64, out[2] tests escalated
+ * to exact expansions, out[3] cells deferred to the 256-slot pass, out[4] BVH
+ * nodes visited, out[5] leaves visited, out[6] clips that changed a cell,
+ * out[7] candidates that reached the vertex test. No reference counterpart
+ * (the reference only prints timings, voronoi_ultra.cu:196-219). */
+int pg_stats(const void *workspace, int64_t num_points, uint64_t *out, int32_t count, void *stream);
+
+/* Profile of the last pg_build + pg_emit_adjacency on this thread:
+ * out[0] kernel launches, out[1] LBVH ms, out[2] cell pass ms, out[3] deferred-cell
+ * pass ms, out[4] CSR count + scan ms, out[5] deferred cells, out[6] cell-pass chunks.
+ * The times are recorded only when options->debug != 0 (CUDA events on the stream).
+ * No reference counterpart (the reference prints timings with debug=True,
+ * voronoi_ultra.cu:196-219, 368-373). */
+int pg_last_profile(double *out, int32_t count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PARAGRAM_B200_H */

@@ -1,0 +1,64 @@
+"""ctypes binding of libparagram_b200.so (the C ABI declared in include/paragram_b200.h)."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libparagram_b200.so")
+
+_lock = threading.Lock()
+_lib = None
+
+
+class PgOptions(ctypes.Structure):
+    """Mirror of ``pg_options`` (include/paragram_b200.h)."""
+
+    _fields_ = [
+        ("knn", ctypes.c_int32),
+        ("leaf_size", ctypes.c_int32),
+        ("debug", ctypes.c_int32),
+        ("num_chunks", ctypes.c_int32),
+    ]
+
+
+#: Symbols declared in include/paragram_b200.h.
+EXPORTED = ["pg_version", "pg_last_error", "pg_workspace_size", "pg_build", "pg_emit_adjacency", "pg_stats",
+            "pg_last_profile"]
+
+
+def load() -> ctypes.CDLL:
+    """Load the CUDA library; raise ImportError when it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                "paragram_b200 CUDA library is missing (libparagram_b200.so); build it with "
+                "`python -m paragram_b200.build` (nvcc with sm_100a support is required)"
+            )
+        lib = ctypes.CDLL(LIB_PATH)
+        vp, i64, i32, sz = ctypes.c_void_p, ctypes.c_int64, ctypes.c_int32, ctypes.c_size_t
+        lib.pg_version.restype = ctypes.c_int
+        lib.pg_last_error.restype = ctypes.c_char_p
+        lib.pg_workspace_size.argtypes = [i64, ctypes.POINTER(sz)]
+        lib.pg_workspace_size.restype = ctypes.c_int
+        lib.pg_build.argtypes = [i64, vp, vp, vp, vp, ctypes.POINTER(PgOptions), vp, sz, vp, vp,
+                                 ctypes.POINTER(i64), vp]
+        lib.pg_build.restype = ctypes.c_int
+        lib.pg_emit_adjacency.argtypes = [i64, vp, vp, vp, vp]
+        lib.pg_emit_adjacency.restype = ctypes.c_int
+        lib.pg_stats.argtypes = [vp, i64, ctypes.POINTER(ctypes.c_uint64), i32, vp]
+        lib.pg_stats.restype = ctypes.c_int
+        lib.pg_last_profile.argtypes = [ctypes.POINTER(ctypes.c_double), i32]
+        lib.pg_last_profile.restype = ctypes.c_int
+        _lib = lib
+        return lib
+
+
+def last_error(lib: ctypes.CDLL) -> str:
+    msg = lib.pg_last_error()
+    return msg.decode() if msg else ""

@@ -1,0 +1,79 @@
+"""Build recipe of libparagram_b200.so (sm_100a, in-tree).
+
+Every ``csrc/*.cu`` file is compiled by nvcc for ``sm_100a`` and linked into
+``paragram_b200/libparagram_b200.so`` next to this file, so the library
+travels with the source tree. Object files go to ``paragram_b200/_build/``.
+"""
+
+from __future__ import annotations
+
+import concurrent.futures
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD_DIR = os.path.join(HERE, "_build")
+LIB_PATH = os.path.join(HERE, "libparagram_b200.so")
+SOURCES = ["pg_api.cu", "pg_lbvh.cu", "pg_cells.cu", "pg_csr.cu", "pg_scan.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _deps() -> list[str]:
+    return [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))] + [
+        os.path.join(HERE, "..", "include", "paragram_b200.h")
+    ]
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB_PATH):
+        return False
+    t = os.path.getmtime(LIB_PATH)
+    return all(os.path.getmtime(d) <= t for d in _deps() if os.path.exists(d))
+
+
+def _compile(src: str, ptxas_verbose: bool) -> tuple[str, str]:
+    obj = os.path.join(BUILD_DIR, os.path.splitext(src)[0] + ".o")
+    cmd = [nvcc(), *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+    if ptxas_verbose:
+        cmd += ["-Xptxas", "-v"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src}:\n{r.stderr}")
+    return obj, r.stderr
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
+    """Compile the CUDA library for sm_100a if it is missing or stale."""
+    if not force and up_to_date():
+        return LIB_PATH
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
+        results = list(ex.map(lambda s: _compile(s, ptxas_verbose), SOURCES))
+    if verbose or ptxas_verbose:
+        for _, log in results:
+            if log:
+                print(log, file=sys.stderr)
+    objs = [o for o, _ in results]
+    tmp = LIB_PATH + ".tmp"
+    cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"nvcc link failed:\n{r.stderr}")
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, ptxas_verbose="--ptxas" in sys.argv)
+    print(LIB_PATH)

@@ -1,0 +1,328 @@
+// pg_api.cu -- C ABI (include/paragram_b200.h) and host orchestration.
+//
+// Reference orchestration: build_voronoi_ultra (voronoi_ultra.cu:143-376) and
+// build_laguerre_voronoi_ultra (laguerre_ultra.cu:176-454):
+// pack -> BVH + kNN -> chunked cell kernel -> gather -> symmetrise -> cumsum
+// -> populate. Here: LBVH -> chunked cell launches -> deferred-cell pass ->
+// CSR count + scan (offsets) -> [host reads E] -> CSR fill.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "../../include/paragram_b200.h"
+#include "pg_common.cuh"
+#include "pg_kernels.cuh"
+
+namespace pg
+{
+
+static thread_local std::string g_last_error;
+thread_local long long g_launches = 0;
+static thread_local double g_profile[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+
+static int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static int64_t big_cap(int64_t n) { return std::min<int64_t>(n, 65536 + n / 32); }
+
+size_t workspace_layout(int64_t n, char *base, Workspace *ws)
+{
+    size_t off = 0;
+    auto take = [&](size_t bytes) -> char * {
+        char *p = base ? base + off : nullptr;
+        off += align_up(bytes);
+        return p;
+    };
+    size_t N = (size_t)std::max<int64_t>(n, 1);
+    int blocks = sort_blocks((int64_t)N);
+    size_t hist_elems = (size_t)256 * blocks + 1;
+    size_t scan_elems = scan_tmp_elems((int64_t)std::max(hist_elems, N + 1));
+    Workspace w;
+    w.bounds = (int *)take(8 * sizeof(int));
+    w.box = (float *)take(8 * sizeof(float));
+    w.morton = (float *)take(4 * sizeof(float));
+    w.counters = (int *)take(16 * sizeof(int));
+    w.stats = (unsigned long long *)take(kNumStats * sizeof(unsigned long long));
+    w.keys0 = (unsigned long long *)take(8 * N);
+    w.keys1 = (unsigned long long *)take(8 * N);
+    w.vals0 = (uint32_t *)take(4 * N);
+    w.vals1 = (uint32_t *)take(4 * N);
+    w.hist = (uint32_t *)take(4 * hist_elems);
+    w.scan_tmp = (uint32_t *)take(4 * scan_elems);
+    w.pts = (float4 *)take(16 * N);
+    w.oid = (int *)take(4 * N);
+    w.rank = (int *)take(4 * N);
+    w.left = (int *)take(4 * N);
+    w.right = (int *)take(4 * N);
+    w.first = (int *)take(4 * N);
+    w.last = (int *)take(4 * N);
+    w.parent_int = (int *)take(4 * N);
+    w.parent_leaf = (int *)take(4 * N);
+    w.flags = (int *)take(4 * N);
+    w.nbox = (float4 *)take(32 * N);
+    w.records = (float4 *)take(64 * N);
+    w.rows = (int *)take(4 * N * kRowWidth);
+    w.deg = (int *)take(4 * N);
+    w.big_list = (int *)take(4 * N);
+    w.big_rows = (int *)take(4 * (size_t)big_cap((int64_t)N) * kBigRowWidth);
+    w.big_slabs = take(big_slab_bytes());
+    w.tslabs = take(tcell_slab_bytes());
+    w.cnt = (int *)take(4 * N);
+    w.miss = (int *)take(4 * N);
+    w.fill = (int *)take(4 * N);
+    w.sizes = (uint32_t *)take(4 * (N + 1));
+    w.bytes = off;
+    if (ws)
+        *ws = w;
+    return off;
+}
+
+// Chunk plan of the cell pass. Mirrors plan_convex_cell_chunks (chunking.h:16-56):
+// PARAGRAM_NUM_CHUNKS forces a count; otherwise the per-cell scratch is compared
+// with PARAGRAM_MEM_FRAC (0.05 < f < 0.95, default 0.5) of the free device
+// memory. The clipper keeps its per-cell polyhedron in shared memory, so its
+// only per-cell global scratch is the directed row (kRowWidth ints).
+static int plan_chunks(int64_t n, int requested)
+{
+    if (requested > 0)
+        return requested;
+    const char *force = std::getenv("PARAGRAM_NUM_CHUNKS");
+    if (force && std::atoi(force) > 0)
+        return std::atoi(force);
+    double frac = 0.5;
+    const char *fe = std::getenv("PARAGRAM_MEM_FRAC");
+    if (fe)
+    {
+        double f = std::atof(fe);
+        if (f > 0.05 && f < 0.95)
+            frac = f;
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return 1;
+    }
+    size_t full = (size_t)n * kRowWidth * sizeof(int);
+    size_t budget = (size_t)(frac * (double)free_b);
+    if (budget > 0 && full > budget)
+        return (int)((full + budget - 1) / budget);
+    return 1;
+}
+
+static int device_sms()
+{
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaGetLastError();
+    return sms;
+}
+
+} // namespace pg
+
+extern "C" {
+
+int pg_version(void) { return 100; }
+
+const char *pg_last_error(void) { return pg::g_last_error.c_str(); }
+
+int pg_workspace_size(int64_t num_points, size_t *bytes)
+{
+    if (!bytes)
+        return pg::fail(PG_ERR_INVALID, "bytes must not be NULL");
+    if (num_points < 0 || num_points >= pg::kMaxPoints)
+        return pg::fail(PG_ERR_INVALID, "num_points must be in [0, 2^26)");
+    *bytes = pg::workspace_layout(num_points, nullptr, nullptr);
+    return PG_OK;
+}
+
+int pg_build(int64_t n, const float *points, const float *weights, const int32_t *guesses, const int32_t *guess_off,
+             const pg_options *options, void *workspace, size_t workspace_bytes, int32_t *offsets, int32_t *status,
+             int64_t *num_edges, void *stream)
+{
+    using namespace pg;
+    g_last_error.clear();
+    cudaStream_t st = (cudaStream_t)stream;
+    pg_options opt = {8, -1, 0, 0};
+    if (options)
+        opt = *options;
+    if (n < 0 || n >= kMaxPoints)
+        return fail(PG_ERR_INVALID, "num_points must be in [0, 2^26)");
+    if (!num_edges || !offsets)
+        return fail(PG_ERR_INVALID, "offsets and num_edges must not be NULL");
+    if ((guesses == nullptr) != (guess_off == nullptr))
+        return fail(PG_ERR_INVALID, "initial_guesses and initial_guesses_offsets must be provided together");
+    if (n > 0 && (!points || !status || !workspace))
+        return fail(PG_ERR_INVALID, "points, status and workspace must not be NULL");
+    if (((uintptr_t)workspace & 255u) != 0)
+        return fail(PG_ERR_INVALID, "workspace must be 256-byte aligned");
+    if (opt.leaf_size > kMaxLeaf)
+        return fail(PG_ERR_INVALID, "leaf_size must be at most 32");
+    size_t need = workspace_layout(n, nullptr, nullptr);
+    if (workspace_bytes < need)
+        return fail(PG_ERR_INVALID, "workspace too small: need " + std::to_string(need) + " bytes");
+    cudaGetLastError();
+    if (n == 0)
+    {
+        cudaMemsetAsync(offsets, 0, sizeof(int32_t), st);
+        *num_edges = 0;
+        cudaError_t e = cudaStreamSynchronize(st);
+        return e == cudaSuccess ? PG_OK : fail(PG_ERR_CUDA, cudaGetErrorString(e));
+    }
+    Workspace ws;
+    workspace_layout(n, (char *)workspace, &ws);
+    int leaf = opt.leaf_size > 0 ? opt.leaf_size : kDefaultLeaf;
+    g_launches = 0;
+    for (double &v : g_profile)
+        v = 0.0;
+    // debug bit 0: print phase timings (reference behaviour); bit 1: record them for pg_last_profile
+    const bool timing = opt.debug != 0;
+    cudaEvent_t ev[5];
+    if (timing)
+        for (auto &e : ev)
+            cudaEventCreate(&e);
+    if (timing)
+        cudaEventRecord(ev[0], st);
+    cudaMemsetAsync(ws.counters, 0, 16 * sizeof(int), st);
+    cudaMemsetAsync(ws.stats, 0, kNumStats * sizeof(unsigned long long), st);
+    lbvh_build(ws, n, points, weights, leaf, st);
+    if (timing)
+        cudaEventRecord(ev[1], st);
+    CellLaunch cl;
+    cl.n = n;
+    cl.leaf_size = leaf;
+    cl.root = n == 1 ? leaf_ref(0, 1) : (n <= leaf ? leaf_ref(0, (int)n) : 0);
+    cl.window = (guesses == nullptr && opt.knn > 0) ? kWindow : 0;
+    cl.guesses = guesses;
+    cl.guess_off = guess_off;
+    cl.weighted = weights != nullptr;
+    {
+        const char *mb = std::getenv("PG_CELL_MIN_BLOCKS");
+        cl.min_blocks = mb ? std::atoi(mb) : 2; // 2: warp per cell (default); 0: thread per cell
+        const char *pf = std::getenv("PG_PROFILE");
+        cl.prof = pf ? std::atoi(pf) : 0;
+    }
+    int chunks = plan_chunks(n, opt.num_chunks);
+    int sms = device_sms();
+    int64_t per = (n + chunks - 1) / chunks;
+    for (int c = 0; c < chunks; ++c)
+    {
+        cl.cell_begin = (int64_t)c * per;
+        cl.cell_end = std::min<int64_t>(n, cl.cell_begin + per);
+        if (cl.cell_begin >= cl.cell_end)
+            break;
+        cells_launch(ws, cl, status, sms, st);
+    }
+    if (timing)
+        cudaEventRecord(ev[4], st);
+    cells_big_launch(ws, cl, status, big_cap(n), st);
+    if (timing)
+        cudaEventRecord(ev[2], st);
+    csr_count(ws, n, offsets, st);
+    int host[4] = {0, 0, 0, 0};
+    int64_t edges = 0;
+    {
+        uint32_t e32 = 0;
+        cudaMemcpyAsync(&e32, offsets + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(host, ws.counters, 4 * sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaError_t e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+            return fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+        edges = e32;
+    }
+    if (timing)
+    {
+        cudaEventRecord(ev[3], st);
+        cudaEventSynchronize(ev[3]);
+        float t_bvh = 0, t_cells = 0, t_fast = 0, t_csr = 0;
+        cudaEventElapsedTime(&t_bvh, ev[0], ev[1]);
+        cudaEventElapsedTime(&t_cells, ev[1], ev[2]);
+        cudaEventElapsedTime(&t_fast, ev[1], ev[4]);
+        cudaEventElapsedTime(&t_csr, ev[2], ev[3]);
+        g_profile[1] = t_bvh;
+        g_profile[2] = t_fast;
+        g_profile[3] = t_cells - t_fast;
+        g_profile[4] = t_csr;
+        if (opt.debug & 1)
+        {
+            std::printf("BVH Creation time: %f ms\n", t_bvh);
+            std::printf("Cell construction time: %f ms (%d chunk(s), %d deferred cell(s))\n", t_cells, chunks,
+                        host[1]);
+            std::printf("CSR count time: %f ms\n", t_csr);
+        }
+        for (auto &e : ev)
+            cudaEventDestroy(e);
+    }
+    g_profile[0] = (double)g_launches;
+    g_profile[5] = (double)host[1];
+    g_profile[6] = (double)chunks;
+    if (host[2] != 0)
+        return fail(PG_ERR_INTERNAL, "exact predicate exceeded its expansion capacity");
+    if (host[1] > big_cap(n))
+        return fail(PG_ERR_INTERNAL, "too many cells exceeded 64 vertices (" + std::to_string(host[1]) +
+                                         " > capacity " + std::to_string(big_cap(n)) + ")");
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    *num_edges = edges;
+    return PG_OK;
+}
+
+int pg_emit_adjacency(int64_t n, const void *workspace, const int32_t *offsets, int32_t *adjacency, void *stream)
+{
+    using namespace pg;
+    g_last_error.clear();
+    if (n < 0 || n >= kMaxPoints)
+        return fail(PG_ERR_INVALID, "num_points must be in [0, 2^26)");
+    if (n == 0)
+        return PG_OK;
+    if (!workspace || !offsets || !adjacency)
+        return fail(PG_ERR_INVALID, "workspace, offsets and adjacency must not be NULL");
+    Workspace ws;
+    workspace_layout(n, (char *)workspace, &ws);
+    long long before = g_launches;
+    csr_fill(ws, n, offsets, adjacency, (cudaStream_t)stream);
+    g_profile[0] += (double)(g_launches - before);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    return PG_OK;
+}
+
+int pg_last_profile(double *out, int32_t count)
+{
+    if (!out || count < 0)
+        return pg::fail(PG_ERR_INVALID, "bad arguments");
+    for (int i = 0; i < count && i < 8; ++i)
+        out[i] = pg::g_profile[i];
+    return PG_OK;
+}
+
+int pg_stats(const void *workspace, int64_t n, uint64_t *out, int32_t count, void *stream)
+{
+    using namespace pg;
+    if (!workspace || !out || count < 0)
+        return fail(PG_ERR_INVALID, "bad arguments");
+    Workspace ws;
+    workspace_layout(n, (char *)workspace, &ws);
+    unsigned long long tmp[kNumStats];
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaMemcpyAsync(tmp, ws.stats, sizeof(tmp), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return fail(PG_ERR_CUDA, cudaGetErrorString(e));
+    for (int i = 0; i < count && i < kNumStats; ++i)
+        out[i] = tmp[i];
+    return PG_OK;
+}
+
+} // extern "C"

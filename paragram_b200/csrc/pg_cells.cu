@@ -1,0 +1,1531 @@
+// pg_cells.cu -- per-cell convex clipping, one warp per cell.
+//
+// Reference counterpart: compute_bvh_voronoi_kernel (voronoi_ultra.cu:39-141)
+// and compute_bvh_power_diagram_kernel (laguerre_ultra.cu:43-174): one thread
+// per cell, polyhedron state in a strided global scratch (ConvexCellMemory,
+// faster_convex_cell.cuh:33-70), clipping by CCClipByPlane
+// (faster_convex_cell.cuh:411-512) during a shrinking-radius BVH traversal
+// (pwr_bvh.cuh:217-356).
+//
+// Here one warp owns a cell. The polyhedron lives in shared memory
+// (struct CellMem: planes, vertices, plane ids, traversal stack); lanes own
+// vertex slots (slot = k * 32 + lane). Candidates come in batches of up to 32
+// (one per lane): the warm-start window of curve-order neighbours, the
+// caller's initial guesses, then BVH leaves. A batch is filtered by a
+// security-radius test, then by an FP32 vertex test with a rigorous error
+// bound; the surviving candidates clip one at a time, nearest first:
+//   1. every lane classifies its vertices (FP32 filter; undecided tests go to
+//      the exact cascade of pg_exact.cuh);
+//   2. the removed vertices' triangles (in the dual: each vertex is a triangle
+//      of its three planes) give the boundary edges of the new face: a
+//      directed edge x->y of a removed triangle whose reverse is not an edge
+//      of another removed triangle; each boundary edge x->y makes the new
+//      vertex (P, x, y) -- the reference builds the same cycle sequentially
+//      in CCComputeBoundary (faster_convex_cell.cuh:322-388);
+//   3. new vertices fill the freed slots (ballot / popc ranks), are computed
+//      in FP32 by Cramer's rule with an a-posteriori error bound (residuals of
+//      the exact planes at the computed point times ||A^-1||).
+// A BVH node is visited only if some vertex v could be removed by a point of
+// the node's box: dist(v, box)^2 < |v - s|^2 + (max weight in box - w_s),
+// tested lane-parallel over the vertices.
+//
+// A cell that needs more than 64 vertex / plane slots or 64 stack entries is
+// deferred to a second pass with 256 slots in global memory; its status is
+// then vertex_overflow (2) if the final cell has more than 64 vertices (the
+// reference MAX_VERTS) and plane_overflow (1) only if even 256 slots overflow.
+#include <cfloat>
+#include <climits>
+
+#include "pg_common.cuh"
+#include "pg_exact.cuh"
+#include "pg_kernels.cuh"
+
+namespace pg
+{
+
+constexpr float kEps = 5.9604645e-8f; // 2^-24
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+template <int CAP, int STACK> struct CellMem
+{
+    float4 pl[CAP];   // plane (n.x, n.y, n.z, h): interior n.x <= h (relative to the seed)
+    float4 vx[CAP];   // vertex (X.x, X.y, X.z, psi), psi bounds the FP32 side-test error
+    float pe[CAP];    // bound on |h - h_exact|
+    float vr[CAP];    // (|X| + psi)^2, upper bound on |X_exact|^2
+    int pid[CAP];     // >= 0: sorted point index; < 0: -1 - box code
+    unsigned vt[CAP]; // plane slots p0 | p1 << 8 | p2 << 16 (oriented)
+    unsigned eb[CAP]; // boundary edges x | y << 8 of the clip in progress, by rank
+    int stk[STACK];
+    unsigned long long cnt[kNumStats]; // per-warp statistics (written by lane 0)
+};
+
+struct CellArgs
+{
+    const float4 *pts;
+    const int *oid;
+    const int *rank;
+    const float4 *rec;
+    const float *box;
+    int n;
+    int root;
+    int window;
+    const int *guesses;
+    const int *guess_off;
+    int *rows;
+    int *deg;
+    int *status;
+    int *big_list;
+    int *big_rows;
+    int *counters;
+    unsigned long long *stats;
+    int64_t begin, end;
+    int big_pass;
+    int64_t big_cap;
+    char *slabs;
+    int prof; // accumulate per-phase clock64() cycles into the statistics
+};
+
+enum Flag : int
+{
+    kFlagEmpty = 1,
+    kFlagDefer = 2,
+    kFlagError = 4,
+};
+
+template <int CAP> struct WarpState
+{
+    static constexpr int W = CAP / 32;
+    unsigned valid[W];
+    int np;
+    float4 s;
+    int si, soid;
+    float rsafe;
+    int flags;
+};
+
+// statistics live in the warp's shared-memory block, not in registers
+// The value is evaluated by every lane (it may contain warp-collective calls).
+#define PG_COUNT(m, lane, idx, v)                                                                                      \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        unsigned long long pg_count_v_ = (unsigned long long)(v);                                                      \
+        if ((lane) == 0)                                                                                               \
+            (m).cnt[idx] += pg_count_v_;                                                                               \
+    } while (0)
+#define PG_TIC(A, v) long long v = (A).prof ? clock64() : 0
+#define PG_TOC(A, m, lane, slot, v)                                                                                    \
+    if ((A).prof && (lane) == 0)                                                                                       \
+    (m).cnt[kStatCycCell + (slot)] += (unsigned long long)(clock64() - v)
+
+struct Cand
+{
+    float nx, ny, nz, h;
+    float nrm;  // upper bound on |q - s|
+    float cerr; // constant part of the side-test error bound
+    float eh;   // bound on |h - h_exact|
+    int id;     // sorted index
+};
+
+__device__ __forceinline__ Cand make_cand(float4 s, float4 q, int id)
+{
+    Cand c;
+    c.nx = q.x - s.x;
+    c.ny = q.y - s.y;
+    c.nz = q.z - s.z;
+    float n2 = __fmaf_rn(c.nx, c.nx, __fmaf_rn(c.ny, c.ny, __fmul_rn(c.nz, c.nz)));
+    float dw = q.w - s.w;
+    c.h = 0.5f * __fsub_rn(n2, dw);
+    c.eh = 2.0f * kEps * (fabsf(c.h) + 3.0f * n2 + fabsf(dw));
+    c.nrm = __fsqrt_rn(n2) * (1.0f + 8.0f * kEps);
+    c.cerr = (3.0f * kEps * fabsf(c.h) + c.eh) * (1.0f + 8.0f * kEps);
+    if (!(n2 > 1e-30f && n2 < 1e30f))
+        c.cerr = INFINITY; // out of the filter's range: always exact
+    c.id = id;
+    return c;
+}
+
+__device__ __forceinline__ Cand shfl_cand(const Cand &c, int src)
+{
+    Cand r;
+    r.nx = __shfl_sync(kFull, c.nx, src);
+    r.ny = __shfl_sync(kFull, c.ny, src);
+    r.nz = __shfl_sync(kFull, c.nz, src);
+    r.h = __shfl_sync(kFull, c.h, src);
+    r.nrm = __shfl_sync(kFull, c.nrm, src);
+    r.cerr = __shfl_sync(kFull, c.cerr, src);
+    r.eh = __shfl_sync(kFull, c.eh, src);
+    r.id = __shfl_sync(kFull, c.id, src);
+    return r;
+}
+
+// +1 removed, 0 kept, -1 undecided
+__device__ __forceinline__ int side_fp32(float4 X, const Cand &q)
+{
+    float g = __fmaf_rn(q.nx, X.x, __fmaf_rn(q.ny, X.y, __fmaf_rn(q.nz, X.z, -q.h)));
+    float b = __fmaf_rn(q.nrm, X.w, q.cerr) * (1.0f + 1e-6f);
+    return g > b ? 1 : (g < -b ? 0 : -1);
+}
+
+__device__ __forceinline__ exact::PlaneSrc plane_src(int pid, const CellArgs &A)
+{
+    exact::PlaneSrc r;
+    if (pid >= 0)
+    {
+        float4 p = A.pts[pid];
+        r.x = p.x;
+        r.y = p.y;
+        r.z = p.z;
+        r.w = p.w;
+        r.box = -1;
+        r.oid = A.oid[pid];
+    }
+    else
+    {
+        int code = -1 - pid;
+        r.x = A.box[(code & 1) * 3 + (code >> 1)];
+        r.y = r.z = r.w = 0.0f;
+        r.box = code;
+        r.oid = -1;
+    }
+    return r;
+}
+
+// Exact cascade for one undecided test. Takes plain values so that no
+// per-warp state has its address taken (which would move it to local memory).
+__device__ __noinline__ int side_exact(int p0, int p1, int p2, int qid, const float4 *__restrict__ pts,
+                                       const int *__restrict__ oid, const float *__restrict__ box, float4 s, int soid,
+                                       int *used)
+{
+    CellArgs A;
+    A.pts = pts;
+    A.oid = oid;
+    A.box = box;
+    exact::PlaneSrc vp[3] = {plane_src(p0, A), plane_src(p1, A), plane_src(p2, A)};
+    exact::PlaneSrc cp = plane_src(qid, A);
+    return exact::side_test(vp, cp, s.x, s.y, s.z, s.w, soid, used);
+}
+
+// Vertex of three planes (FP32 Cramer) with its side-test error radius psi.
+__device__ __forceinline__ float4 make_vertex(float4 a, float ea, float4 b, float eb, float4 c, float ec, float &vr)
+{
+    float u0x = b.y * c.z - b.z * c.y, u0y = b.z * c.x - b.x * c.z, u0z = b.x * c.y - b.y * c.x;
+    float u1x = c.y * a.z - c.z * a.y, u1y = c.z * a.x - c.x * a.z, u1z = c.x * a.y - c.y * a.x;
+    float u2x = a.y * b.z - a.z * b.y, u2y = a.z * b.x - a.x * b.z, u2z = a.x * b.y - a.y * b.x;
+    float D = a.x * u0x + a.y * u0y + a.z * u0z;
+    float nx = a.w * u0x + b.w * u1x + c.w * u2x;
+    float ny = a.w * u0y + b.w * u1y + c.w * u2y;
+    float nz = a.w * u0z + b.w * u1z + c.w * u2z;
+    float X = __fdiv_rn(nx, D), Y = __fdiv_rn(ny, D), Z = __fdiv_rn(nz, D);
+    float xn = __fsqrt_rn(X * X + Y * Y + Z * Z);
+    float la = fabsf(a.x) + fabsf(a.y) + fabsf(a.z);
+    float lb = fabsf(b.x) + fabsf(b.y) + fabsf(b.z);
+    float lc = fabsf(c.x) + fabsf(c.y) + fabsf(c.z);
+    float ra = fabsf(__fmaf_rn(a.x, X, __fmaf_rn(a.y, Y, __fmaf_rn(a.z, Z, -a.w)))) + 4.0f * kEps * (la * xn + fabsf(a.w)) + ea;
+    float rb = fabsf(__fmaf_rn(b.x, X, __fmaf_rn(b.y, Y, __fmaf_rn(b.z, Z, -b.w)))) + 4.0f * kEps * (lb * xn + fabsf(b.w)) + eb;
+    float rc = fabsf(__fmaf_rn(c.x, X, __fmaf_rn(c.y, Y, __fmaf_rn(c.z, Z, -c.w)))) + 4.0f * kEps * (lc * xn + fabsf(c.w)) + ec;
+    float rho = sqrtf(ra * ra + rb * rb + rc * rc);
+    float F = sqrtf(u0x * u0x + u0y * u0y + u0z * u0z + u1x * u1x + u1y * u1y + u1z * u1z + u2x * u2x + u2y * u2y +
+                    u2z * u2z) +
+              8.0f * kEps * (lb * lc + lc * la + la * lb);
+    float den = fabsf(D) - 8.0f * kEps * la * lb * lc;
+    float ex = den > 0.0f ? F * rho / den : INFINITY;
+    float psi = (2.0f * ex + 4.0f * kEps * xn) * (1.0f + 1e-6f);
+    if (!(psi < 1e30f) || !(xn < 1e30f))
+        psi = INFINITY;
+    float r = xn + psi;
+    vr = r * r * (1.0f + 1e-6f);
+    return make_float4(X, Y, Z, psi);
+}
+
+template <int CAP, int STACK>
+__device__ __forceinline__ void cell_init(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, const CellArgs &A, int lane)
+{
+    // 6 box planes (code = axis * 2 + side, side 1 = high face)
+    if (lane < 6)
+    {
+        int ax = lane >> 1, hi = lane & 1;
+        float sc = ax == 0 ? ws.s.x : (ax == 1 ? ws.s.y : ws.s.z);
+        float b = A.box[hi * 3 + ax];
+        float h = hi ? __fsub_rn(b, sc) : __fsub_rn(sc, b);
+        float sg = hi ? 1.0f : -1.0f;
+        m.pl[lane] = make_float4(ax == 0 ? sg : 0.0f, ax == 1 ? sg : 0.0f, ax == 2 ? sg : 0.0f, h);
+        m.pe[lane] = kEps * fabsf(h);
+        m.pid[lane] = -1 - lane;
+    }
+    __syncwarp();
+    // 8 corners; triples ordered so the outward normals have a positive triple product
+    if (lane < 8)
+    {
+        int sx = lane & 1, sy = (lane >> 1) & 1, sz = (lane >> 2) & 1;
+        int px = sx, py = 2 + sy, pz = 4 + sz;
+        int sign = (sx ? 1 : -1) * (sy ? 1 : -1) * (sz ? 1 : -1);
+        int p0 = sign > 0 ? px : py, p1 = sign > 0 ? py : px, p2 = pz;
+        float vr;
+        m.vx[lane] = make_vertex(m.pl[p0], m.pe[p0], m.pl[p1], m.pe[p1], m.pl[p2], m.pe[p2], vr);
+        m.vr[lane] = vr;
+        m.vt[lane] = (unsigned)p0 | ((unsigned)p1 << 8) | ((unsigned)p2 << 16);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < WarpState<CAP>::W; ++k)
+        ws.valid[k] = k == 0 ? 0xFFu : 0u;
+    ws.np = 6;
+    ws.flags = 0;
+    float vr = lane < 8 ? m.vr[lane] : 0.0f;
+    ws.rsafe = sqrtf(__uint_as_float(__reduce_max_sync(kFull, __float_as_uint(vr)))) * (1.0f + 1e-6f);
+}
+
+template <int W> __device__ __forceinline__ int count_bits(const unsigned (&m)[W])
+{
+    int c = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        c += __popc(m[k]);
+    return c;
+}
+
+// Drop planes no valid vertex references; renumber vertex triples.
+template <int CAP, int STACK> __device__ __forceinline__ void gc_planes(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int lane)
+{
+    constexpr int W = CAP / 32;
+    unsigned lm[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        lm[k] = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        if ((ws.valid[k] >> lane) & 1u)
+        {
+            unsigned t = m.vt[k * 32 + lane];
+            unsigned p[3] = {t & 255u, (t >> 8) & 255u, (t >> 16) & 255u};
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+#pragma unroll
+                for (int kk = 0; kk < W; ++kk)
+                    if ((int)(p[e] >> 5) == kk)
+                        lm[kk] |= 1u << (p[e] & 31u);
+        }
+    unsigned live[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        live[k] = __reduce_or_sync(kFull, lm[k]);
+    int pre[W];
+    int acc = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+    {
+        pre[k] = acc;
+        acc += __popc(live[k]);
+    }
+    float4 tpl[W];
+    float tpe[W];
+    int tpid[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+    {
+        int p = k * 32 + lane;
+        if (p < ws.np && ((live[k] >> lane) & 1u))
+        {
+            tpl[k] = m.pl[p];
+            tpe[k] = m.pe[p];
+            tpid[k] = m.pid[p];
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+    {
+        int p = k * 32 + lane;
+        if (p < ws.np && ((live[k] >> lane) & 1u))
+        {
+            int q = pre[k] + __popc(live[k] & ((1u << lane) - 1u));
+            m.pl[q] = tpl[k];
+            m.pe[q] = tpe[k];
+            m.pid[q] = tpid[k];
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        if ((ws.valid[k] >> lane) & 1u)
+        {
+            unsigned t = m.vt[k * 32 + lane];
+            unsigned out = 0;
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+            {
+                unsigned p = (t >> (8 * e)) & 255u;
+                unsigned q = 0;
+#pragma unroll
+                for (int kk = 0; kk < W; ++kk)
+                    if ((int)(p >> 5) == kk)
+                        q = pre[kk] + __popc(live[kk] & ((1u << (p & 31u)) - 1u));
+                out |= q << (8 * e);
+            }
+            m.vt[k * 32 + lane] = out;
+        }
+    ws.np = acc;
+    __syncwarp();
+}
+
+enum ClipResult : int
+{
+    kClipNone = 0,
+    kClipChanged = 1,
+    kClipEmptied = 2,
+    kClipDefer = 3,
+};
+
+template <int CAP, int STACK>
+__device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, const Cand &q, const CellArgs &A, int lane)
+{
+    constexpr int W = CAP / 32;
+    unsigned rem[W];
+    unsigned tri[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+    {
+        int r = 0;
+        tri[k] = 0;
+        if ((ws.valid[k] >> lane) & 1u)
+        {
+            int slot = k * 32 + lane;
+            float4 X = m.vx[slot];
+            r = side_fp32(X, q);
+            if (r < 0)
+            {
+                unsigned t = m.vt[slot];
+                int used = 0;
+                r = side_exact(m.pid[t & 255u], m.pid[(t >> 8) & 255u], m.pid[(t >> 16) & 255u], q.id, A.pts, A.oid,
+                               A.box, ws.s, ws.soid, &used);
+                atomicAdd(&m.cnt[kStatFp64], 1ull);
+                if (used)
+                    atomicAdd(&m.cnt[kStatExpansion], 1ull);
+                if (r < 0)
+                {
+                    ws.flags |= kFlagError;
+                    r = 0;
+                }
+            }
+            if (r)
+                tri[k] = m.vt[slot];
+        }
+        rem[k] = __ballot_sync(kFull, r == 1);
+    }
+    PG_COUNT(m, lane, kStatTests, count_bits(ws.valid));
+    bool any = false, all = true;
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+    {
+        any = any || rem[k] != 0u;
+        all = all && rem[k] == ws.valid[k];
+    }
+    if (!any)
+        return kClipNone;
+    if (all)
+    {
+        ws.flags |= kFlagEmpty;
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            ws.valid[k] = 0;
+        return kClipEmptied;
+    }
+    if (ws.np >= CAP)
+    {
+        gc_planes(m, ws, lane);
+        if (ws.np >= CAP)
+            return kClipDefer;
+        // plane slots were renumbered: reload the removed triangles
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+            if ((rem[k] >> lane) & 1u)
+                tri[k] = m.vt[k * 32 + lane];
+    }
+    int P = ws.np++;
+    if (lane == 0)
+    {
+        m.pl[P] = make_float4(q.nx, q.ny, q.nz, q.h);
+        m.pe[P] = q.eh;
+        m.pid[P] = q.id;
+    }
+    // boundary edges of the removed region
+    unsigned bf = 0; // bit k*3+e: edge e of my removed vertex in word k is a boundary edge
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        if ((rem[k] >> lane) & 1u)
+            bf |= 7u << (3 * k);
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+    {
+        unsigned mm = rem[k];
+        while (mm)
+        {
+            int b = __ffs(mm) - 1;
+            mm &= mm - 1;
+            unsigned t = __shfl_sync(kFull, tri[k], b);
+            unsigned t0 = t & 255u, t1 = (t >> 8) & 255u, t2 = (t >> 16) & 255u;
+#pragma unroll
+            for (int kk = 0; kk < W; ++kk)
+            {
+                unsigned my = tri[kk];
+                unsigned m0 = my & 255u, m1 = (my >> 8) & 255u, m2 = (my >> 16) & 255u;
+                unsigned xs[3] = {m0, m1, m2}, ys[3] = {m1, m2, m0};
+#pragma unroll
+                for (int e = 0; e < 3; ++e)
+                {
+                    unsigned x = xs[e], y = ys[e];
+                    bool rev = (t0 == y && t1 == x) || (t1 == y && t2 == x) || (t2 == y && t0 == x);
+                    if (rev)
+                        bf &= ~(1u << (3 * kk + e));
+                }
+            }
+        }
+    }
+    // list the boundary edges by rank in the warp's edge buffer
+    const unsigned lt = (1u << lane) - 1u;
+    int nb = 0;
+#pragma unroll
+    for (int f = 0; f < 3 * W; ++f)
+    {
+        unsigned bal = __ballot_sync(kFull, (bf >> f) & 1u);
+        if ((bf >> f) & 1u)
+        {
+            unsigned my = tri[f / 3];
+            unsigned x = (my >> (8 * (f % 3))) & 255u;
+            unsigned y = (my >> (8 * ((f % 3 + 1) % 3))) & 255u;
+            m.eb[nb + __popc(bal & lt)] = x | (y << 8);
+        }
+        nb += __popc(bal);
+    }
+    int nv_new = count_bits(ws.valid) - count_bits(rem) + nb;
+    if (nv_new > CAP)
+        return kClipDefer;
+    unsigned fr[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        fr[k] = ~ws.valid[k] | rem[k];
+    __syncwarp(); // edge list, plane P and all reads of removed triangles are done
+    float4 pP = m.pl[P];
+    float eP = m.pe[P];
+    unsigned nbits[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        nbits[k] = 0;
+    // lane r builds the vertex (P, x, y) of the r-th boundary edge in the r-th free slot
+    for (int r0 = 0; r0 < nb; r0 += 32)
+    {
+        int r = r0 + lane;
+        if (r < nb)
+        {
+            unsigned xy = m.eb[r];
+            unsigned x = xy & 255u, y = xy >> 8;
+            int rr = r, slot = -1;
+#pragma unroll
+            for (int k = 0; k < W; ++k)
+            {
+                int c = __popc(fr[k]);
+                if (slot < 0 && rr < c)
+                    slot = k * 32 + (int)__fns(fr[k], 0, rr + 1);
+                else if (slot < 0)
+                    rr -= c;
+            }
+            if (slot >= 0 && slot < CAP)
+            {
+                float vr;
+                float4 X = make_vertex(pP, eP, m.pl[x], m.pe[x], m.pl[y], m.pe[y], vr);
+                m.vx[slot] = X;
+                m.vr[slot] = vr;
+                m.vt[slot] = (unsigned)P | (x << 8) | (y << 16);
+#pragma unroll
+                for (int k = 0; k < W; ++k)
+                    if ((slot >> 5) == k)
+                        nbits[k] |= 1u << (slot & 31);
+            }
+            else
+                ws.flags |= kFlagError; // unreachable: capacity was checked above
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        ws.valid[k] = (ws.valid[k] & ~rem[k]) | __reduce_or_sync(kFull, nbits[k]);
+    __syncwarp();
+    PG_COUNT(m, lane, kStatClips, 1);
+    return kClipChanged;
+}
+
+template <int CAP, int STACK> __device__ __forceinline__ void update_rsafe(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int lane)
+{
+    float mx = 0.0f;
+#pragma unroll
+    for (int k = 0; k < CAP / 32; ++k)
+        if ((ws.valid[k] >> lane) & 1u)
+            mx = fmaxf(mx, m.vr[k * 32 + lane]);
+    ws.rsafe = sqrtf(__uint_as_float(__reduce_max_sync(kFull, __float_as_uint(mx)))) * (1.0f + 1e-6f);
+}
+
+// Process one batch of candidates (one per lane, `have` marks real ones).
+// Returns false when the cell is finished early (empty or deferred).
+template <int CAP, int STACK>
+__device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, bool have, const Cand &q, float key,
+                          const CellArgs &A, int lane)
+{
+    // security radius: no vertex can be removed when h - eh > |a| * rsafe
+    if (have && (q.h - q.eh) > q.nrm * ws.rsafe * (1.0f + 1e-6f))
+        have = false;
+    if (__ballot_sync(kFull, have) == 0u)
+        return true;
+    unsigned nhave = __popc(__ballot_sync(kFull, have));
+    PG_COUNT(m, lane, kStatCandidates, nhave);
+    unsigned todo = __ballot_sync(kFull, have);
+    bool changed = false;
+    while (todo)
+    {
+        unsigned kk = ((todo >> lane) & 1u) ? ((__float_as_uint(key) & ~31u) | (unsigned)lane) : 0xFFFFFFFFu;
+        unsigned mn = __reduce_min_sync(kFull, kk);
+        int src = (int)(mn & 31u);
+        todo &= ~(1u << src);
+        Cand c = shfl_cand(q, src);
+        PG_TIC(A, tc);
+        int r = clip(m, ws, c, A, lane);
+        PG_TOC(A, m, lane, 4, tc);
+        if (r == kClipEmptied)
+            return false;
+        if (r == kClipDefer)
+        {
+            ws.flags |= kFlagDefer;
+            return false;
+        }
+        changed = changed || r == kClipChanged;
+    }
+    if (changed)
+        update_rsafe(m, ws, lane);
+    return true;
+}
+
+// Can a point of this box (with max weight mw) remove a vertex of the cell?
+template <int CAP, int STACK>
+__device__ __forceinline__ bool node_may_clip(const CellMem<CAP, STACK> &m, const WarpState<CAP> &ws, float lx, float ly,
+                                              float lz, float hx, float hy, float hz, float mw, int lane, float &d2out)
+{
+    float rlx = lx - ws.s.x, rly = ly - ws.s.y, rlz = lz - ws.s.z;
+    float rhx = hx - ws.s.x, rhy = hy - ws.s.y, rhz = hz - ws.s.z;
+    float dx = fmaxf(fmaxf(rlx, -rhx), 0.0f), dy = fmaxf(fmaxf(rly, -rhy), 0.0f), dz = fmaxf(fmaxf(rlz, -rhz), 0.0f);
+    float d2 = (dx * dx + dy * dy + dz * dz) * (1.0f - 1e-6f);
+    d2out = d2;
+    float dm = mw - ws.s.w;
+    float R2 = ws.rsafe * ws.rsafe * (1.0f + 1e-5f);
+    if (dm <= 0.0f)
+    {
+        if (d2 > 4.0f * R2)
+            return false;
+    }
+    else
+    {
+        float num = d2 - dm * (1.0f + 1e-6f);
+        if (num > 0.0f && num * num > 4.0f * d2 * R2)
+            return false;
+    }
+    float dmu = dm > 0.0f ? dm * (1.0f + 1e-6f) : dm * (1.0f - 1e-6f);
+    bool may = false;
+#pragma unroll
+    for (int k = 0; k < CAP / 32; ++k)
+        if ((ws.valid[k] >> lane) & 1u)
+        {
+            int slot = k * 32 + lane;
+            float4 X = m.vx[slot];
+            float e = X.w + 1e-6f * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z) + fabsf(rlx) + fabsf(rly) + fabsf(rlz) +
+                                     fabsf(rhx) + fabsf(rhy) + fabsf(rhz));
+            float ax = fmaxf(fmaxf(rlx - e - X.x, X.x - rhx - e), 0.0f);
+            float ay = fmaxf(fmaxf(rly - e - X.y, X.y - rhy - e), 0.0f);
+            float az = fmaxf(fmaxf(rlz - e - X.z, X.z - rhz - e), 0.0f);
+            float lhs = (ax * ax + ay * ay + az * az) * (1.0f - 1e-6f);
+            if (lhs < m.vr[slot] + dmu)
+                may = true;
+        }
+    return __ballot_sync(kFull, may) != 0u;
+}
+
+// Returns false when the row does not fit the fast-pass row width (the cell
+// is then deferred to the large-capacity pass).
+template <int CAP, int STACK>
+__device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, const CellArgs &A, int lane)
+{
+    constexpr int W = CAP / 32;
+    int oi = ws.soid;
+    if (ws.flags & kFlagEmpty)
+    {
+        if (lane == 0)
+        {
+            A.deg[oi] = 0;
+            A.status[oi] = kEmptyCell;
+        }
+        return true;
+    }
+    unsigned lm[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        lm[k] = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        if ((ws.valid[k] >> lane) & 1u)
+        {
+            unsigned t = m.vt[k * 32 + lane];
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+            {
+                unsigned p = (t >> (8 * e)) & 255u;
+#pragma unroll
+                for (int kk = 0; kk < W; ++kk)
+                    if ((int)(p >> 5) == kk)
+                        lm[kk] |= 1u << (p & 31u);
+            }
+        }
+    int o[W];
+    unsigned has[W];
+    int cnt = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+    {
+        unsigned live = __reduce_or_sync(kFull, lm[k]);
+        int p = k * 32 + lane;
+        o[k] = INT_MAX;
+        if (p < ws.np && ((live >> lane) & 1u))
+        {
+            int id = m.pid[p];
+            if (id >= 0)
+                o[k] = A.oid[id];
+        }
+        has[k] = __ballot_sync(kFull, o[k] != INT_MAX);
+        cnt += __popc(has[k]);
+    }
+    int rnk[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        rnk[k] = 0;
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+    {
+        unsigned mm = has[k];
+        while (mm)
+        {
+            int b = __ffs(mm) - 1;
+            mm &= mm - 1;
+            int v = __shfl_sync(kFull, o[k], b);
+#pragma unroll
+            for (int kk = 0; kk < W; ++kk)
+                rnk[kk] += (v < o[kk]);
+        }
+    }
+    if (!A.big_pass && cnt > kRowWidth)
+        return false;
+    int nverts = count_bits(ws.valid);
+    int st = nverts > kMaxVertsRef ? kVertexOverflow : kSuccess;
+    if (ws.flags & kFlagDefer)
+        st = kPlaneOverflow; // only reachable in the large-capacity pass
+    int *row;
+    if (A.big_pass)
+    {
+        int bi = ws.si; // index in the deferred list
+        row = A.big_rows + (size_t)bi * kBigRowWidth;
+        if (lane == 0)
+        {
+            A.rows[(size_t)oi * kRowWidth] = bi;
+            A.deg[oi] = cnt | (int)kBigFlag;
+        }
+    }
+    else
+    {
+        row = A.rows + (size_t)oi * kRowWidth;
+        if (lane == 0)
+            A.deg[oi] = cnt;
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+        if (o[k] != INT_MAX)
+            row[rnk[k]] = o[k];
+    if (lane == 0)
+        A.status[oi] = st;
+    return true;
+}
+
+template <int CAP, int STACK>
+__device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int i, const CellArgs &A, int lane)
+{
+    ws.s = A.pts[i];
+    ws.si = i;
+    ws.soid = A.oid[i];
+    cell_init(m, ws, A, lane);
+    const int n = A.n;
+    const bool guessing = A.guesses != nullptr;
+    PG_TIC(A, tw);
+    // 1. warm start: curve-order neighbours (or the caller's initial guesses)
+    if (guessing)
+    {
+        int g0 = A.guess_off[ws.soid], g1 = A.guess_off[ws.soid + 1];
+        for (int g = g0; g < g1; g += 32)
+        {
+            int j = -1;
+            if (g + lane < g1)
+            {
+                int o = A.guesses[g + lane];
+                if (o >= 0 && o < n)
+                    j = A.rank[o];
+            }
+            bool have = j >= 0 && j != i;
+            Cand q;
+            float key = 0.0f;
+            if (have)
+            {
+                float4 p = A.pts[j];
+                have = !(p.x == ws.s.x && p.y == ws.s.y && p.z == ws.s.z);
+                q = make_cand(ws.s, p, j);
+                key = q.nrm;
+                for (int t = 0; t < ws.np && have; ++t)
+                    have = m.pid[t] != j;
+            }
+            // deduplicate within the batch: keep the first lane holding a point
+            unsigned peers = __match_any_sync(kFull, have ? j : -2 - lane);
+            if (have && (__ffs(peers) - 1) != lane)
+                have = false;
+            if (!run_batch(m, ws, have, q, key, A, lane))
+                return;
+        }
+    }
+    else if (A.window > 0)
+    {
+        int off = lane < A.window ? lane - A.window : lane - A.window + 1;
+        int j = i + off;
+        bool have = lane < 2 * A.window && j >= 0 && j < n;
+        Cand q;
+        float key = 0.0f;
+        if (have)
+        {
+            float4 p = A.pts[j];
+            have = !(p.x == ws.s.x && p.y == ws.s.y && p.z == ws.s.z);
+            q = make_cand(ws.s, p, j);
+            key = q.nrm;
+        }
+        if (!run_batch(m, ws, have, q, key, A, lane))
+            return;
+    }
+    PG_TOC(A, m, lane, 1, tw);
+    // 2. BVH traversal, nearest child first
+    int sp = 0;
+    if (lane == 0)
+        m.stk[0] = A.root;
+    sp = 1;
+    __syncwarp();
+    while (sp > 0)
+    {
+        int ref = m.stk[--sp];
+        if (ref_is_leaf(ref))
+        {
+            PG_COUNT(m, lane, kStatLeaves, 1);
+            int first = leaf_first(ref), count = leaf_count(ref);
+            int j = first + lane;
+            bool have = lane < count && j != i;
+            if (have && !guessing && A.window > 0 && j >= i - A.window && j <= i + A.window)
+                have = false;
+            Cand q;
+            float key = 0.0f;
+            if (have)
+            {
+                float4 p = A.pts[j];
+                have = !(p.x == ws.s.x && p.y == ws.s.y && p.z == ws.s.z);
+                q = make_cand(ws.s, p, j);
+                key = q.nrm;
+                if (guessing)
+                    for (int t = 0; t < ws.np && have; ++t)
+                        have = m.pid[t] != j;
+            }
+            PG_TIC(A, tl);
+            bool go = run_batch(m, ws, have, q, key, A, lane);
+            PG_TOC(A, m, lane, 3, tl);
+            if (!go)
+                return;
+            continue;
+        }
+        PG_COUNT(m, lane, kStatNodes, 1);
+        PG_TIC(A, tn);
+        const float4 *r = A.rec + 4 * (size_t)ref;
+        float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+        float d0, d1;
+        bool c0 = node_may_clip(m, ws, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r3.z, lane, d0);
+        bool c1 = node_may_clip(m, ws, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.w, lane, d1);
+        int ref0 = __float_as_int(r3.x), ref1 = __float_as_int(r3.y);
+        PG_TOC(A, m, lane, 2, tn);
+        if (sp + 2 > STACK)
+        {
+            ws.flags |= kFlagDefer;
+            return;
+        }
+        __syncwarp();
+        if (c0 && c1)
+        {
+            int nearr = d0 <= d1 ? ref0 : ref1, farr = d0 <= d1 ? ref1 : ref0;
+            if (lane == 0)
+            {
+                m.stk[sp] = farr;
+                m.stk[sp + 1] = nearr;
+            }
+            sp += 2;
+        }
+        else if (c0 || c1)
+        {
+            if (lane == 0)
+                m.stk[sp] = c0 ? ref0 : ref1;
+            sp += 1;
+        }
+        __syncwarp();
+    }
+}
+
+template <int CAP, int STACK> __device__ void flush_stats(CellMem<CAP, STACK> &m, const CellArgs &A, int lane)
+{
+    __syncwarp();
+    if (lane < kNumStats && m.cnt[lane])
+        atomicAdd(&A.stats[lane], m.cnt[lane]);
+}
+
+template <int CAP, int STACK>
+__device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArgs &A, int lane)
+{
+    WarpState<CAP> ws;
+    if (lane < kNumStats)
+        m.cnt[lane] = 0;
+    __syncwarp();
+    int64_t count = A.big_pass ? min((int64_t)A.counters[1], A.big_cap) : (A.end - A.begin);
+    int *ctr = A.big_pass ? &A.counters[3] : &A.counters[0];
+    for (;;)
+    {
+        int t = 0;
+        if (lane == 0)
+            t = atomicAdd(ctr, 1);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= count)
+            break;
+        int i = A.big_pass ? A.big_list[t] : (int)(A.begin + t);
+        PG_TIC(A, tcell);
+        process_cell(m, ws, i, A, lane);
+        if (A.big_pass)
+            ws.si = t; // the deferred-row slot
+        if (ws.flags & kFlagError)
+        {
+            if (lane == 0)
+                atomicExch(&A.counters[2], 1);
+            ws.flags &= ~kFlagError;
+        }
+        if (!(ws.flags & kFlagDefer) || A.big_pass)
+        {
+            PG_TIC(A, to);
+            bool ok = write_outputs(m, ws, A, lane);
+            PG_TOC(A, m, lane, 5, to);
+            PG_TOC(A, m, lane, 0, tcell);
+            if (ok)
+                continue;
+        }
+        // deferred: placeholder outputs (an empty row) until the large-capacity pass
+        if (lane == 0)
+        {
+            A.deg[ws.soid] = 0;
+            A.status[ws.soid] = kPlaneOverflow;
+            int d = atomicAdd(&A.counters[1], 1);
+            A.big_list[d] = i;
+            atomicAdd(&A.stats[kStatDeferred], 1ull);
+        }
+    }
+    flush_stats(m, A, lane);
+}
+
+template <int MINB> __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) k_cells_fast(CellArgs A)
+{
+    __shared__ CellMem<kCapFast, kStackFast> mem[kWarpsPerBlock];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    cells_body(mem[w], A, lane);
+}
+
+__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_cells_big(CellArgs A)
+{
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    size_t gw = (size_t)blockIdx.x * kWarpsPerBlock + w;
+    auto *m = reinterpret_cast<CellMem<kCapBig, kStackBig> *>(A.slabs + gw * sizeof(CellMem<kCapBig, kStackBig>));
+    cells_body(*m, A, lane);
+}
+
+// ===========================================================================
+// Thread-per-cell fast path.
+//
+// One thread owns a cell (the reference's decomposition, voronoi_ultra.cu:51),
+// so a warp advances 32 neighbouring cells (curve order) at once. The cell
+// lives in a per-warp slab of global memory laid out [slot][lane] (a warp's
+// 32 threads touching the same slot read 32 consecutive elements), cached in
+// L1. The polyhedron is kept compact: vertices [0, nv), planes [0, np).
+// Node and point pruning use the directional corner radius of the cell's
+// conservative bounding box (the reference's get_directional_safety_radius,
+// voronoi_bvh.cuh:71-107, here with rounding margins so that it never prunes
+// a point that could remove a vertex). Cells that need more than kTCap
+// slots or kTStack stack entries are deferred to the 256-slot warp pass.
+// ===========================================================================
+constexpr int kTCap = 64;
+constexpr int kTStack = 64;
+constexpr int kTMaxBoundary = 48;
+
+struct TSlab
+{
+    float4 pl[kTCap][32];
+    float4 vx[kTCap][32];
+    float pe[kTCap][32];
+    int pid[kTCap][32];
+    unsigned vt[kTCap][32];
+};
+
+struct TCell
+{
+    float4 s;
+    int si, soid;
+    int nv, np;
+    float lx, ly, lz, ux, uy, uz; // bounding box of the exact cell, relative to the seed
+    int flags;
+};
+
+__device__ __forceinline__ void t_bounds(const TSlab &S, int lane, TCell &c)
+{
+    float lx = INFINITY, ly = INFINITY, lz = INFINITY, ux = -INFINITY, uy = -INFINITY, uz = -INFINITY;
+    for (int j = 0; j < c.nv; ++j)
+    {
+        float4 X = S.vx[j][lane];
+        lx = fminf(lx, X.x - X.w);
+        ly = fminf(ly, X.y - X.w);
+        lz = fminf(lz, X.z - X.w);
+        ux = fmaxf(ux, X.x + X.w);
+        uy = fmaxf(uy, X.y + X.w);
+        uz = fmaxf(uz, X.z + X.w);
+    }
+    // the subtractions / additions above round: widen by a relative margin
+    c.lx = lx - 1e-6f * fabsf(lx);
+    c.ly = ly - 1e-6f * fabsf(ly);
+    c.lz = lz - 1e-6f * fabsf(lz);
+    c.ux = ux + 1e-6f * fabsf(ux);
+    c.uy = uy + 1e-6f * fabsf(uy);
+    c.uz = uz + 1e-6f * fabsf(uz);
+}
+
+// squared corner radius of the cell box over the octants allowed per axis
+__device__ __forceinline__ float t_axis_r2(float lo_rel, float hi_rel, float L, float U)
+{
+    float neg = fmaxf(-L, 0.0f), pos = fmaxf(U, 0.0f);
+    float a = lo_rel <= 0.0f ? neg * neg : 0.0f;
+    float b = hi_rel >= 0.0f ? pos * pos : 0.0f;
+    return fmaxf(a, b);
+}
+
+// Can a point of box [lo, hi] (absolute) with max weight mw remove a vertex?
+__device__ __forceinline__ bool t_box_may_clip(const TCell &c, float lx, float ly, float lz, float hx, float hy,
+                                               float hz, float mw)
+{
+    float rlx = lx - c.s.x, rly = ly - c.s.y, rlz = lz - c.s.z;
+    float rhx = hx - c.s.x, rhy = hy - c.s.y, rhz = hz - c.s.z;
+    float dx = fmaxf(rlx, 0.0f) + fmaxf(-rhx, 0.0f);
+    float dy = fmaxf(rly, 0.0f) + fmaxf(-rhy, 0.0f);
+    float dz = fmaxf(rlz, 0.0f) + fmaxf(-rhz, 0.0f);
+    float d2 = (dx * dx + dy * dy + dz * dz) * (1.0f - 1e-5f);
+    float r2 = (t_axis_r2(rlx, rhx, c.lx, c.ux) + t_axis_r2(rly, rhy, c.ly, c.uy) + t_axis_r2(rlz, rhz, c.lz, c.uz)) *
+               (1.0f + 1e-5f);
+    float dm = mw - c.s.w;
+    if (dm <= 0.0f)
+        return !(d2 > 4.0f * r2);
+    float num = d2 - dm * (1.0f + 1e-5f);
+    if (num <= 0.0f)
+        return true;
+    return !(num * num > 4.0f * d2 * r2);
+}
+
+// Can candidate q (plane n.x = h) remove a vertex? Directional corner test.
+__device__ __forceinline__ bool t_cand_may_clip(const TCell &c, const Cand &q)
+{
+    float ax = q.nx, ay = q.ny, az = q.nz;
+    float r2 = t_axis_r2(ax, ax, c.lx, c.ux) + t_axis_r2(ay, ay, c.ly, c.uy) + t_axis_r2(az, az, c.lz, c.uz);
+    float hm = q.h - q.eh; // lower bound of the exact h
+    if (hm <= 0.0f)
+        return true;
+    float n2 = q.nrm * q.nrm; // upper bound of |a|^2
+    return !(hm * hm > n2 * r2 * (1.0f + 1e-5f));
+}
+
+__device__ __forceinline__ void t_init(TSlab &S, int lane, TCell &c, const CellArgs &A)
+{
+    for (int code = 0; code < 6; ++code)
+    {
+        int ax = code >> 1, hi = code & 1;
+        float sc = ax == 0 ? c.s.x : (ax == 1 ? c.s.y : c.s.z);
+        float b = A.box[hi * 3 + ax];
+        float h = hi ? __fsub_rn(b, sc) : __fsub_rn(sc, b);
+        float sg = hi ? 1.0f : -1.0f;
+        S.pl[code][lane] = make_float4(ax == 0 ? sg : 0.0f, ax == 1 ? sg : 0.0f, ax == 2 ? sg : 0.0f, h);
+        S.pe[code][lane] = kEps * fabsf(h);
+        S.pid[code][lane] = -1 - code;
+    }
+    for (int k = 0; k < 8; ++k)
+    {
+        int sx = k & 1, sy = (k >> 1) & 1, sz = (k >> 2) & 1;
+        int px = sx, py = 2 + sy, pz = 4 + sz;
+        int sign = (sx ? 1 : -1) * (sy ? 1 : -1) * (sz ? 1 : -1);
+        int p0 = sign > 0 ? px : py, p1 = sign > 0 ? py : px, p2 = pz;
+        float vr;
+        S.vx[k][lane] =
+            make_vertex(S.pl[p0][lane], S.pe[p0][lane], S.pl[p1][lane], S.pe[p1][lane], S.pl[p2][lane], S.pe[p2][lane], vr);
+        S.vt[k][lane] = (unsigned)p0 | ((unsigned)p1 << 8) | ((unsigned)p2 << 16);
+    }
+    c.nv = 8;
+    c.np = 6;
+    c.flags = 0;
+    t_bounds(S, lane, c);
+}
+
+// drop planes no vertex references (vertices keep their slots)
+__device__ __noinline__ int t_gc(TSlab &S, int lane, int nv, int np)
+{
+    unsigned long long live = 0;
+    for (int j = 0; j < nv; ++j)
+    {
+        unsigned t = S.vt[j][lane];
+        live |= (1ull << (t & 255u)) | (1ull << ((t >> 8) & 255u)) | (1ull << ((t >> 16) & 255u));
+    }
+    int w = 0;
+    for (int p = 0; p < np; ++p)
+        if ((live >> p) & 1ull)
+        {
+            if (w != p)
+            {
+                S.pl[w][lane] = S.pl[p][lane];
+                S.pe[w][lane] = S.pe[p][lane];
+                S.pid[w][lane] = S.pid[p][lane];
+            }
+            ++w;
+        }
+    for (int j = 0; j < nv; ++j)
+    {
+        unsigned t = S.vt[j][lane], out = 0;
+        for (int e = 0; e < 3; ++e)
+        {
+            unsigned p = (t >> (8 * e)) & 255u;
+            unsigned q = __popcll(live & ((1ull << p) - 1ull));
+            out |= q << (8 * e);
+        }
+        S.vt[j][lane] = out;
+    }
+    return w;
+}
+
+__device__ __forceinline__ bool tri_has_edge(unsigned u, unsigned a, unsigned b)
+{
+    unsigned u0 = u & 255u, u1 = (u >> 8) & 255u, u2 = (u >> 16) & 255u;
+    return (u0 == a && u1 == b) || (u1 == a && u2 == b) || (u2 == a && u0 == b);
+}
+
+__device__ __forceinline__ int t_clip(TSlab &S, int lane, TCell &c, const Cand &q, const CellArgs &A,
+                                      unsigned &n_fp64, unsigned &n_exp)
+{
+    unsigned long long rm = 0;
+    for (int j = 0; j < c.nv; ++j)
+    {
+        int r = side_fp32(S.vx[j][lane], q);
+        if (r < 0)
+        {
+            unsigned t = S.vt[j][lane];
+            int used = 0;
+            r = side_exact(S.pid[t & 255u][lane], S.pid[(t >> 8) & 255u][lane], S.pid[(t >> 16) & 255u][lane], q.id,
+                           A.pts, A.oid, A.box, c.s, c.soid, &used);
+            ++n_fp64;
+            n_exp += used;
+            if (r < 0)
+            {
+                c.flags |= kFlagError;
+                r = 0;
+            }
+        }
+        if (r)
+            rm |= 1ull << j;
+    }
+    if (!rm)
+        return kClipNone;
+    int R = __popcll(rm);
+    if (R == c.nv)
+    {
+        c.flags |= kFlagEmpty;
+        c.nv = 0;
+        return kClipEmptied;
+    }
+    if (c.np >= kTCap)
+    {
+        c.np = t_gc(S, lane, c.nv, c.np);
+        if (c.np >= kTCap)
+            return kClipDefer;
+    }
+    int P = c.np++;
+    S.pl[P][lane] = make_float4(q.nx, q.ny, q.nz, q.h);
+    S.pe[P][lane] = q.eh;
+    S.pid[P][lane] = q.id;
+    // boundary edges of the removed region
+    unsigned short be[kTMaxBoundary];
+    int nb = 0;
+    for (unsigned long long m1 = rm; m1; m1 &= m1 - 1ull)
+    {
+        int j = __ffsll((long long)m1) - 1;
+        unsigned t = S.vt[j][lane];
+        unsigned tv[3] = {t & 255u, (t >> 8) & 255u, (t >> 16) & 255u};
+        for (int e = 0; e < 3; ++e)
+        {
+            unsigned x = tv[e], y = tv[(e + 1) % 3];
+            bool interior = false;
+            for (unsigned long long m2 = rm; m2 && !interior; m2 &= m2 - 1ull)
+            {
+                int k = __ffsll((long long)m2) - 1;
+                interior = k != j && tri_has_edge(S.vt[k][lane], y, x);
+            }
+            if (!interior)
+            {
+                if (nb >= kTMaxBoundary)
+                    return kClipDefer;
+                be[nb++] = (unsigned short)(x | (y << 8));
+            }
+        }
+    }
+    int keepn = c.nv - R;
+    if (keepn + nb > kTCap)
+        return kClipDefer;
+    // compact: kept vertices at or above keepn move into the holes below keepn
+    unsigned long long low = keepn >= 64 ? ~0ull : ((1ull << keepn) - 1ull);
+    unsigned long long all = c.nv >= 64 ? ~0ull : ((1ull << c.nv) - 1ull);
+    unsigned long long holes = rm & low;
+    unsigned long long src = (all & ~rm) & ~low;
+    while (holes)
+    {
+        int j = __ffsll((long long)holes) - 1, k = __ffsll((long long)src) - 1;
+        holes &= holes - 1ull;
+        src &= src - 1ull;
+        S.vx[j][lane] = S.vx[k][lane];
+        S.vt[j][lane] = S.vt[k][lane];
+    }
+    float4 pP = S.pl[P][lane];
+    float eP = S.pe[P][lane];
+    for (int b = 0; b < nb; ++b)
+    {
+        unsigned x = be[b] & 255u, y = be[b] >> 8;
+        float vr;
+        S.vx[keepn + b][lane] = make_vertex(pP, eP, S.pl[x][lane], S.pe[x][lane], S.pl[y][lane], S.pe[y][lane], vr);
+        S.vt[keepn + b][lane] = (unsigned)P | (x << 8) | (y << 16);
+    }
+    c.nv = keepn + nb;
+    return kClipChanged;
+}
+
+struct TStats
+{
+    unsigned tests, fp64, exp, nodes, leaves, clips, cands;
+};
+
+// returns false when the cell finished early (empty / deferred)
+__device__ __forceinline__ bool t_try(TSlab &S, int lane, TCell &c, int j, const CellArgs &A, TStats &ts, bool &changed)
+{
+    float4 p = A.pts[j];
+    if (p.x == c.s.x && p.y == c.s.y && p.z == c.s.z)
+        return true; // coincident points never clip each other
+    Cand q = make_cand(c.s, p, j);
+    if (!t_cand_may_clip(c, q))
+        return true;
+    ++ts.cands;
+    ts.tests += c.nv;
+    int r = t_clip(S, lane, c, q, A, ts.fp64, ts.exp);
+    if (r == kClipEmptied)
+        return false;
+    if (r == kClipDefer)
+    {
+        c.flags |= kFlagDefer;
+        return false;
+    }
+    if (r == kClipChanged)
+    {
+        ++ts.clips;
+        changed = true;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void t_process(TSlab &S, int lane, TCell &c, const CellArgs &A, TStats &ts)
+{
+    t_init(S, lane, c, A);
+    const int n = A.n, i = c.si;
+    const bool guessing = A.guesses != nullptr;
+    bool changed = false;
+    if (guessing)
+    {
+        int g0 = A.guess_off[c.soid], g1 = A.guess_off[c.soid + 1];
+        for (int g = g0; g < g1; ++g)
+        {
+            int o = A.guesses[g];
+            if (o < 0 || o >= n)
+                continue;
+            int j = A.rank[o];
+            if (j == i)
+                continue;
+            bool dup = false;
+            for (int t = 0; t < c.np && !dup; ++t)
+                dup = S.pid[t][lane] == j;
+            if (dup)
+                continue;
+            if (!t_try(S, lane, c, j, A, ts, changed))
+                return;
+        }
+    }
+    else
+    {
+        for (int d = 1; d <= A.window; ++d)
+        {
+            if (i - d >= 0 && !t_try(S, lane, c, i - d, A, ts, changed))
+                return;
+            if (i + d < n && !t_try(S, lane, c, i + d, A, ts, changed))
+                return;
+        }
+    }
+    if (changed)
+        t_bounds(S, lane, c);
+    int stk[kTStack];
+    int sp = 0;
+    stk[sp++] = A.root;
+    while (sp > 0)
+    {
+        int ref = stk[--sp];
+        if (ref_is_leaf(ref))
+        {
+            ++ts.leaves;
+            int first = leaf_first(ref), count = leaf_count(ref);
+            changed = false;
+            for (int l = 0; l < count; ++l)
+            {
+                int j = first + l;
+                if (j == i)
+                    continue;
+                if (!guessing && j >= i - A.window && j <= i + A.window)
+                    continue;
+                if (guessing)
+                {
+                    bool dup = false;
+                    for (int t = 0; t < c.np && !dup; ++t)
+                        dup = S.pid[t][lane] == j;
+                    if (dup)
+                        continue;
+                }
+                if (!t_try(S, lane, c, j, A, ts, changed))
+                    return;
+            }
+            if (changed)
+                t_bounds(S, lane, c);
+            continue;
+        }
+        ++ts.nodes;
+        const float4 *r = A.rec + 4 * (size_t)ref;
+        float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2), r3 = __ldg(r + 3);
+        bool c0 = t_box_may_clip(c, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r3.z);
+        bool c1 = t_box_may_clip(c, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.w);
+        if (sp + 2 > kTStack)
+        {
+            c.flags |= kFlagDefer;
+            return;
+        }
+        int ref0 = __float_as_int(r3.x), ref1 = __float_as_int(r3.y);
+        if (c0 && c1)
+        {
+            // nearer child (by box distance from the seed) on top
+            float d0 = fmaxf(fmaxf(r0.x - c.s.x, c.s.x - r0.w), 0.0f) + fmaxf(fmaxf(r0.y - c.s.y, c.s.y - r1.x), 0.0f) +
+                       fmaxf(fmaxf(r0.z - c.s.z, c.s.z - r1.y), 0.0f);
+            float d1 = fmaxf(fmaxf(r1.z - c.s.x, c.s.x - r2.y), 0.0f) + fmaxf(fmaxf(r1.w - c.s.y, c.s.y - r2.z), 0.0f) +
+                       fmaxf(fmaxf(r2.x - c.s.z, c.s.z - r2.w), 0.0f);
+            stk[sp++] = d0 <= d1 ? ref1 : ref0;
+            stk[sp++] = d0 <= d1 ? ref0 : ref1;
+        }
+        else if (c0)
+            stk[sp++] = ref0;
+        else if (c1)
+            stk[sp++] = ref1;
+    }
+}
+
+__device__ __forceinline__ bool t_write(const TSlab &S, int lane, const TCell &c, const CellArgs &A)
+{
+    int oi = c.soid;
+    if (c.flags & kFlagEmpty)
+    {
+        A.deg[oi] = 0;
+        A.status[oi] = kEmptyCell;
+        return true;
+    }
+    unsigned long long live = 0;
+    for (int j = 0; j < c.nv; ++j)
+    {
+        unsigned t = S.vt[j][lane];
+        live |= (1ull << (t & 255u)) | (1ull << ((t >> 8) & 255u)) | (1ull << ((t >> 16) & 255u));
+    }
+    // box planes have no neighbour (after plane GC they can sit in any slot)
+    for (unsigned long long m = live; m; m &= m - 1ull)
+    {
+        int p = __ffsll((long long)m) - 1;
+        if (S.pid[p][lane] < 0)
+            live &= ~(1ull << p);
+    }
+    int cnt = __popcll(live);
+    if (cnt > kRowWidth)
+        return false;
+    int *row = A.rows + (size_t)oi * kRowWidth;
+    int k = 0;
+    for (unsigned long long m = live; m; m &= m - 1ull)
+    {
+        int p = __ffsll((long long)m) - 1;
+        int o = A.oid[S.pid[p][lane]];
+        // insertion into the sorted prefix row[0..k)
+        int t = k;
+        while (t > 0 && row[t - 1] > o)
+        {
+            row[t] = row[t - 1];
+            --t;
+        }
+        row[t] = o;
+        ++k;
+    }
+    A.deg[oi] = cnt;
+    A.status[oi] = c.nv > kMaxVertsRef ? kVertexOverflow : kSuccess;
+    return true;
+}
+
+__global__ void __launch_bounds__(256, 4) k_tcells(CellArgs A, TSlab *slabs)
+{
+    int lane = threadIdx.x & 31;
+    size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    TSlab &S = slabs[gw];
+    TStats ts = {0, 0, 0, 0, 0, 0, 0};
+    int64_t count = A.end - A.begin;
+    for (;;)
+    {
+        int base = 0;
+        if (lane == 0)
+            base = atomicAdd(&A.counters[0], 32);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= count)
+            break;
+        int t = base + lane;
+        if (t < count)
+        {
+            TCell c;
+            c.si = (int)(A.begin + t);
+            c.s = A.pts[c.si];
+            c.soid = A.oid[c.si];
+            t_process(S, lane, c, A, ts);
+            if (c.flags & kFlagError)
+                atomicExch(&A.counters[2], 1);
+            bool done = !(c.flags & kFlagDefer) && t_write(S, lane, c, A);
+            if (!done)
+            {
+                A.deg[c.soid] = 0;
+                A.status[c.soid] = kPlaneOverflow;
+                int d = atomicAdd(&A.counters[1], 1);
+                A.big_list[d] = c.si;
+                atomicAdd(&A.stats[kStatDeferred], 1ull);
+            }
+        }
+        __syncwarp();
+    }
+    unsigned v[7] = {ts.tests, ts.fp64, ts.exp, ts.nodes, ts.leaves, ts.clips, ts.cands};
+    const int idx[7] = {kStatTests, kStatFp64, kStatExpansion, kStatNodes, kStatLeaves, kStatClips, kStatCandidates};
+#pragma unroll
+    for (int k = 0; k < 7; ++k)
+    {
+        unsigned long long sum = v[k];
+        for (int o = 16; o > 0; o >>= 1)
+            sum += __shfl_down_sync(kFull, sum, o);
+        if (lane == 0 && sum)
+            atomicAdd(&A.stats[idx[k]], sum);
+    }
+}
+
+int tcell_threads() { return 148 * 1024; }
+size_t tcell_slab_bytes() { return sizeof(TSlab) * (size_t)(tcell_threads() / 32); }
+
+int big_warps() { return 148 * kWarpsPerBlock; }
+size_t big_slab_bytes() { return sizeof(CellMem<kCapBig, kStackBig>) * (size_t)big_warps(); }
+
+static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
+{
+    CellArgs A;
+    A.pts = ws.pts;
+    A.oid = ws.oid;
+    A.rank = ws.rank;
+    A.rec = ws.records;
+    A.box = ws.box;
+    A.n = (int)cl.n;
+    A.root = cl.root;
+    A.window = cl.window;
+    A.guesses = cl.guesses;
+    A.guess_off = cl.guess_off;
+    A.rows = ws.rows;
+    A.deg = ws.deg;
+    A.status = nullptr;
+    A.big_list = ws.big_list;
+    A.big_rows = ws.big_rows;
+    A.counters = ws.counters;
+    A.stats = ws.stats;
+    A.begin = cl.cell_begin;
+    A.end = cl.cell_end;
+    A.big_pass = 0;
+    A.big_cap = 0;
+    A.slabs = (char *)ws.big_slabs;
+    A.prof = cl.prof;
+    return A;
+}
+
+void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int num_sms, cudaStream_t st)
+{
+    CellArgs A = make_args(ws, cl);
+    A.status = status;
+    cudaMemsetAsync(ws.counters, 0, sizeof(int), st); // work counter
+    int64_t cells = cl.cell_end - cl.cell_begin;
+    if (cl.min_blocks == 0)
+    {
+        // thread per cell: persistent grid, at most one slab per resident warp
+        int bps = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_tcells, 256, 0);
+        if (bps < 1)
+            bps = 1;
+        int64_t grid = std::min<int64_t>((int64_t)num_sms * bps, tcell_threads() / 256);
+        grid = std::min<int64_t>(grid, (cells + 255) / 256);
+        if (grid < 1)
+            grid = 1;
+        ++g_launches;
+        k_tcells<<<(unsigned)grid, 256, 0, st>>>(A, (TSlab *)ws.tslabs);
+        return;
+    }
+    void (*kern)(CellArgs) = k_cells_fast<2>;
+    int blocks_per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerBlock * 32, 0);
+    if (blocks_per_sm < 1)
+        blocks_per_sm = 1;
+    int64_t grid = (int64_t)num_sms * blocks_per_sm;
+    int64_t need = (cells + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    if (grid > need)
+        grid = need;
+    if (grid < 1)
+        grid = 1;
+    ++g_launches;
+    kern<<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(A);
+}
+
+// The deferred count stays on the device: a fixed grid reads it.
+void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st)
+{
+    CellArgs A = make_args(ws, cl);
+    A.status = status;
+    A.big_pass = 1;
+    A.big_cap = big_cap;
+    ++g_launches;
+    k_cells_big<<<(unsigned)(big_warps() / kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(A);
+}
+
+} // namespace pg

@@ -1,0 +1,42 @@
+// pg_kernels.cuh -- host-side launchers shared between the translation units.
+#pragma once
+
+#include "pg_common.cuh"
+
+namespace pg
+{
+
+// kernel launches issued by the calling thread (reported by pg_last_profile)
+extern thread_local long long g_launches;
+
+// pg_scan.cu
+size_t scan_tmp_elems(int64_t n);
+void exclusive_scan(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *tmp, cudaStream_t st);
+
+// pg_lbvh.cu
+int sort_blocks(int64_t n);
+void lbvh_build(const Workspace &ws, int64_t n, const float *points, const float *weights, int leaf_size,
+                cudaStream_t st);
+
+// pg_cells.cu
+struct CellLaunch
+{
+    int64_t n;
+    int leaf_size;
+    int root;                 // root reference (internal index or leaf code)
+    int window;               // warm-start half width (0: off)
+    const int *guesses;       // initial guesses (original ids) or nullptr
+    const int *guess_off;     // [N+1] offsets of the initial guesses
+    int64_t cell_begin, cell_end; // sorted-slot range of this launch
+    int weighted;
+    int min_blocks; // register-budget variant of the cell kernel (2, 3 or 4 blocks per SM)
+    int prof;       // per-phase cycle counters
+};
+void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int num_sms, cudaStream_t st);
+void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st);
+
+// pg_csr.cu
+void csr_count(const Workspace &ws, int64_t n, int32_t *offsets, cudaStream_t st);
+void csr_fill(const Workspace &ws, int64_t n, const int32_t *offsets, int32_t *adjacency, cudaStream_t st);
+
+} // namespace pg

@@ -1,0 +1,125 @@
+"""Low-level builders, mirroring ``paragram.cuda`` (paragram/cuda/__init__.py:1-12).
+
+``build_voronoi_ultra`` and ``build_laguerre_voronoi_ultra`` take the arguments
+of the reference's pybind functions (paragram/csrc/ext.cpp:10-29) and return the
+tuple ``(adjacency, offsets, status)`` of CUDA int32 tensors. Argument errors
+raise ``RuntimeError`` like the reference's C++ ASSERTs
+(voronoi_ultra.cu:165-173, laguerre_ultra.cu:200-213). Importing this module
+raises ``ImportError`` when the CUDA library is not built, like the
+reference's ``paragram.cuda``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import torch
+
+from .. import _lib
+
+_LIB = _lib.load()
+
+#: Counter names returned by ``last_stats()`` (pg_stats in include/paragram_b200.h).
+STAT_NAMES = ["tests", "fp64_escalations", "exact_escalations", "deferred_cells", "nodes", "leaves", "clips",
+              "candidates", "cyc_cell", "cyc_warm", "cyc_nodes", "cyc_leaves", "cyc_clips", "cyc_out"]
+_last_stats: dict = {}
+#: Names of the values returned by ``last_profile()`` (pg_last_profile in include/paragram_b200.h).
+PROFILE_NAMES = ["launches", "lbvh_ms", "cells_ms", "deferred_ms", "csr_ms", "deferred_cells", "chunks"]
+
+
+def _check(ok: bool, msg: str):
+    if not ok:
+        raise RuntimeError(msg)
+
+
+def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug: bool,
+         initial_guesses: Optional[torch.Tensor], initial_guesses_offsets: Optional[torch.Tensor], leaf_size: int,
+         num_chunks: int = 0, stats: bool = False, profile: bool = False):
+    n = int(points.shape[0])
+    _check(points.device.type == "cuda", "points must be on CUDA device")
+    _check(points.dtype == torch.float32, "points must be of type float")
+    _check(points.dim() == 2 and points.shape[1] == 3, "points must have 3 dimensions")
+    points = points.contiguous()
+    dev = points.device
+    wptr = None
+    if weights is not None:
+        _check(weights.device.type == "cuda", "weights must be on CUDA device")
+        _check(weights.dtype == torch.float32, "weights must be of type float")
+        _check(weights.dim() == 2 and weights.shape[1] == 1, "weights must have 1 dimension")
+        _check(weights.shape[0] == n, "points and weights must have the same number of elements")
+        weights = weights.contiguous()
+        wptr = weights.data_ptr() if n > 0 else None
+    gptr = optr = None
+    if initial_guesses is not None and initial_guesses_offsets is not None:
+        _check(initial_guesses.device.type == "cuda", "initial_guesses must be on CUDA device")
+        _check(initial_guesses_offsets.device.type == "cuda", "initial_guesses_offsets must be on CUDA device")
+        _check(initial_guesses_offsets.shape[0] == n + 1, "initial_guesses_offsets must have size num_points + 1")
+        initial_guesses = initial_guesses.to(torch.int32).contiguous()
+        initial_guesses_offsets = initial_guesses_offsets.to(torch.int32).contiguous()
+        if initial_guesses.numel() == 0:
+            initial_guesses = torch.zeros(1, dtype=torch.int32, device=dev)
+        gptr, optr = initial_guesses.data_ptr(), initial_guesses_offsets.data_ptr()
+    opts = _lib.PgOptions(int(knn), int(leaf_size), int(bool(debug)) | (2 if profile else 0), int(num_chunks))
+    with torch.cuda.device(dev):
+        nbytes = ctypes.c_size_t(0)
+        rc = _LIB.pg_workspace_size(n, ctypes.byref(nbytes))
+        _check(rc == 0, _lib.last_error(_LIB))
+        ws = torch.empty(max(nbytes.value, 1), dtype=torch.uint8, device=dev)
+        offsets = torch.empty(n + 1, dtype=torch.int32, device=dev)
+        status = torch.empty(n, dtype=torch.int32, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        edges = ctypes.c_int64(0)
+        rc = _LIB.pg_build(n, points.data_ptr() if n > 0 else None, wptr, gptr, optr, ctypes.byref(opts),
+                           ws.data_ptr(), nbytes.value, offsets.data_ptr(), status.data_ptr() if n > 0 else None,
+                           ctypes.byref(edges), stream)
+        _check(rc == 0, _lib.last_error(_LIB))
+        adjacency = torch.empty(edges.value, dtype=torch.int32, device=dev)
+        if n > 0:
+            rc = _LIB.pg_emit_adjacency(n, ws.data_ptr(), offsets.data_ptr(),
+                                        adjacency.data_ptr() if edges.value > 0 else offsets.data_ptr(), stream)
+            _check(rc == 0, _lib.last_error(_LIB))
+        if stats and n > 0:
+            out = (ctypes.c_uint64 * len(STAT_NAMES))()
+            rc = _LIB.pg_stats(ws.data_ptr(), n, out, len(STAT_NAMES), stream)
+            _check(rc == 0, _lib.last_error(_LIB))
+            _last_stats.clear()
+            _last_stats.update({k: int(v) for k, v in zip(STAT_NAMES, out)})
+    return adjacency, offsets, status
+
+
+def last_profile() -> dict:
+    """Profile of the last build on this thread (launch count; phase times if it ran with profiling)."""
+    out = (ctypes.c_double * len(PROFILE_NAMES))()
+    _LIB.pg_last_profile(out, len(PROFILE_NAMES))
+    return {k: float(v) for k, v in zip(PROFILE_NAMES, out)}
+
+
+def build_voronoi_ultra(points: torch.Tensor, knn: int = 8, debug: bool = False,
+                        initial_guesses: Optional[torch.Tensor] = None,
+                        initial_guesses_offsets: Optional[torch.Tensor] = None, leaf_size: int = -1):
+    """Unweighted 3D Voronoi adjacency (reference: laguerre.h:24-29)."""
+    return _run(points, None, knn, debug, initial_guesses, initial_guesses_offsets, leaf_size)
+
+
+def build_laguerre_voronoi_ultra(points: torch.Tensor, weights: torch.Tensor, knn: int = 8, debug: bool = False,
+                                 initial_guesses: Optional[torch.Tensor] = None,
+                                 initial_guesses_offsets: Optional[torch.Tensor] = None, leaf_size: int = -1):
+    """Weighted 3D power-diagram adjacency (reference: laguerre.h:13-20)."""
+    return _run(points, weights, knn, debug, initial_guesses, initial_guesses_offsets, leaf_size)
+
+
+def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = None, *, knn: int = 8,
+                     leaf_size: int = -1, num_chunks: int = 0, profile: bool = False,
+                     initial_guesses: Optional[torch.Tensor] = None,
+                     initial_guesses_offsets: Optional[torch.Tensor] = None):
+    """Build and return ``((adjacency, offsets, status), counters)``; counters as in ``STAT_NAMES``."""
+    if weights is not None and weights.dim() == 1:
+        weights = weights[:, None]
+    res = _run(points, weights, knn, False, initial_guesses, initial_guesses_offsets, leaf_size,
+               num_chunks=num_chunks, stats=True, profile=profile)
+    return res, dict(_last_stats)
+
+
+__all__ = ["build_laguerre_voronoi_ultra", "build_voronoi_ultra", "build_with_stats", "last_profile", "STAT_NAMES",
+           "PROFILE_NAMES"]

@@ -1,0 +1,68 @@
+"""The C ABI library loads, exports every symbol of include/paragram_b200.h and
+rejects bad arguments before touching a GPU."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from paragram_b200 import _lib
+
+    return _lib.load()
+
+
+def test_header_symbols_exported(lib):
+    from paragram_b200 import _lib
+
+    header = open(os.path.join(ROOT, "include", "paragram_b200.h")).read()
+    declared = set(re.findall(r"^\s*(?:int|const char \*)\s*(pg_\w+)\s*\(", header, re.M))
+    assert declared == set(_lib.EXPORTED)
+    for name in declared:
+        assert hasattr(lib, name), name
+
+
+def test_version(lib):
+    assert lib.pg_version() >= 100
+
+
+def test_workspace_size(lib):
+    n = ctypes.c_size_t(0)
+    assert lib.pg_workspace_size(1000, ctypes.byref(n)) == 0
+    small = n.value
+    assert lib.pg_workspace_size(1_000_000, ctypes.byref(n)) == 0
+    assert n.value > small > 0
+    assert lib.pg_workspace_size(-1, ctypes.byref(n)) == -1
+    assert lib.pg_workspace_size(1 << 26, ctypes.byref(n)) == -1
+
+
+def _build(lib, n, points=1, weights=None, guesses=None, goff=None, ws=256, ws_bytes=1 << 40, offsets=256,
+           status=256, options=None):
+    from paragram_b200 import _lib
+
+    e = ctypes.c_int64(0)
+    opt = options if options is not None else _lib.PgOptions(8, -1, 0, 0)
+    return lib.pg_build(n, points, weights, guesses, goff, ctypes.byref(opt), ws, ws_bytes, offsets, status,
+                        ctypes.byref(e), None)
+
+
+def test_build_rejects_bad_arguments(lib):
+    from paragram_b200 import _lib
+
+    assert _build(lib, -5) == -1
+    assert _build(lib, 10, points=None) == -1
+    assert _build(lib, 10, ws=None) == -1
+    assert _build(lib, 10, ws=257) == -1  # not 256-byte aligned
+    assert _build(lib, 10, guesses=512) == -1  # guesses without offsets
+    assert _build(lib, 10, ws_bytes=16) == -1  # workspace too small
+    assert _build(lib, 10, options=_lib.PgOptions(8, 64, 0, 0)) == -1  # leaf too large
+    assert "leaf_size" in _lib.last_error(lib)
+
+
+def test_emit_rejects_bad_arguments(lib):
+    assert lib.pg_emit_adjacency(10, None, None, None, None) == -1
