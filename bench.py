@@ -1,0 +1,363 @@
+"""Benchmark: Mcells/s of 3D diagram construction on B200.
+
+Default workload (the headline configuration): Voronoi diagram of N = 5,000,000
+clustered points (90% from 64 truncated isotropic Gaussians, sigma log-uniform
+in [0.005, 0.1], 10% uniform background), seeded synthetic data. One step is
+one full ``paragram_b200.voronoi_diagram`` call (LBVH build, cell clipping,
+CSR) on device-resident points; ``e2e`` repeats the step through the same
+public API from pinned host memory, with the host->device copy of the points
+and the device->host copy of the Diagram inside the timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
+
+For N > 1 (torch.distributed.run, one process per GPU) every rank builds its
+own diagram of an equally sized, differently seeded point set (weak scaling;
+cells shard without any data exchange) and the step time is the max over
+ranks. ``--impl reference`` times the CPU restatement of the reference's
+construction (the parity oracle, all host threads) on a bounded sample of the
+same workload; the reference's CUDA extension cannot be built (its cuBQL
+dependency is not vendored).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_cells_fast_clustered5m.md")
+
+WORKLOADS = {
+    "clustered_voronoi_5m": dict(kind="clustered", n=5_000_000, weighted=False),
+    "uniform_voronoi_100k": dict(kind="uniform", n=100_000, weighted=False),
+    "uniform_power_1m": dict(kind="power", n=1_000_000, weighted=True),
+    "lattice_power_310": dict(kind="lattice", n=310 ** 3, weighted=True),
+}
+
+
+def make_points(spec: dict, seed: int):
+    from paragram_b200 import workloads as W
+
+    k = spec["kind"]
+    if k == "clustered":
+        return W.clustered(spec["n"], seed=seed), None
+    if k == "uniform":
+        return W.uniform(spec["n"], seed=seed), None
+    if k == "power":
+        return W.power_uniform(spec["n"], seed=seed)
+    if k == "lattice":
+        return W.jittered_lattice(round(spec["n"] ** (1 / 3)), seed=seed)
+    raise ValueError(k)
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while active."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._thr = None
+
+    def _run(self):
+        try:
+            p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                  "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                 stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            return
+        try:
+            while not self._stop.is_set():
+                line = p.stdout.readline()
+                if not line:
+                    break
+                self.samples.append([x.strip() for x in line.split(",")])
+        finally:
+            p.kill()
+            p.wait()
+
+    def __enter__(self):
+        self._thr = threading.Thread(target=self._run, daemon=True)
+        self._thr.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._thr.join(timeout=5)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for s in self.samples:
+            try:
+                sm.append(float(s[1]))
+                mx = float(s[2])
+                for k, v in zip(names, s[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(k)
+            except (ValueError, IndexError):
+                continue
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_work(offsets: np.ndarray, weighted: bool) -> tuple[float, float]:
+    """(FP32 flops, compulsory bytes) of a diagram from its output degrees.
+
+    Per cell with degree d: F = d * (20 + 8 * max(8, 2d - 4) + 6 * 38) flops (one
+    clip per final face: bisector, side tests against 2d - 4 vertices, about six
+    new vertices by 3x3 cofactors) and B = 12 + 4 [weighted] + 4 + 4 + 4d bytes
+    (point in, weight in, status and offset out, adjacency out).
+    """
+    d = np.diff(offsets.astype(np.int64)).astype(np.float64)
+    flops = float(np.sum(d * (20.0 + 8.0 * np.maximum(8.0, 2.0 * d - 4.0) + 6.0 * 38.0)))
+    nbytes = float(len(d) * (12 + (4 if weighted else 0) + 8) + 4.0 * d.sum())
+    return flops, nbytes
+
+
+def fp32_peak_tflops(sm_max_mhz: float | None) -> float:
+    """Nominal FP32 (FMA) peak: 148 SMs x 128 lanes x 2 flops x SM clock."""
+    mhz = sm_max_mhz or 1965.0
+    return 148 * 128 * 2 * mhz * 1e6 / 1e12
+
+
+def read_traffic_per_launch() -> float | None:
+    """DRAM bytes per cell-pass launch from the committed ncu summary, if present."""
+    try:
+        for line in open(PROFILE_SUMMARY):
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_oracle_rate(pts, w, sample: int, threads: int = 0) -> dict:
+    from oracle import pg_oracle
+
+    n = pts.shape[0]
+    m = min(sample, n)
+    t0 = time.perf_counter()
+    c = pg_oracle.cells(pts, w, mode="incremental", begin=0, end=m, threads=threads)
+    wall = time.perf_counter() - t0
+    per_cell = c.seconds / max(m, 1)
+    full = c.tree_seconds + per_cell * n
+    return {"value": n / full / 1e6, "cell_rate": m / c.seconds / 1e6, "cores": c.threads, "cells": m,
+            "tree_s": c.tree_seconds, "cells_s": c.seconds, "wall_s": wall}
+
+
+def run_reference(args, spec, rank, world):
+    """CPU restatement of the reference's construction on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    pts, w = make_points(spec, seed=0)
+    sample = args.cpu_sample
+    for _ in range(args.warmup):
+        cpu_oracle_rate(pts, w, max(sample // 10, 1000))
+    vals = []
+    info = None
+    for _ in range(args.steps):
+        info = cpu_oracle_rate(pts, w, sample)
+        vals.append(info["value"])
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference",
+        "metric": "Mcells/s",
+        "value": value,
+        "unit": "Mcells/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * info["wall_s"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "n_points": spec["n"], "weighted": spec["weighted"]},
+        "cpu_baseline": {"value": value, "unit": "Mcells/s", "cores": info["cores"], "kind": "port",
+                         "sample": f"{info['cells']} cells of the {spec['n']}-point workload per step; "
+                                   f"kd-tree over all points ({info['tree_s']:.2f} s) + sampled cells "
+                                   f"({info['cells_s']:.2f} s), extrapolated to all cells"},
+        "e2e": {"value": value, "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CUDA extension not buildable (cuBQL submodule absent); CPU oracle port timed",
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gpu(args, spec, rank, world, local):
+    import torch
+
+    import paragram_b200 as pg
+    import paragram_b200.cuda as pc
+    from paragram_b200 import dist
+
+    dev = torch.device(f"cuda:{local}")
+    torch.cuda.set_device(dev)
+    pts, w = make_points(spec, seed=rank)
+    n = pts.shape[0]
+    h_pts = torch.from_numpy(pts).pin_memory()
+    h_w = torch.from_numpy(w).pin_memory() if w is not None else None
+    d_pts = h_pts.to(dev)
+    d_w = h_w.to(dev) if h_w is not None else None
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+
+    def step_device():
+        if d_w is None:
+            return pc._run(d_pts, None, 8, False, None, None, -1, profile=True)
+        return pc._run(d_pts, d_w[:, None], 8, False, None, None, -1, profile=True)
+
+    def step_e2e():
+        x = h_pts.to(dev, non_blocking=True)
+        if h_w is None:
+            d = pg.voronoi_diagram(x)
+        else:
+            d = pg.power_diagram(x, h_w.to(dev, non_blocking=True))
+        a = d.adjacency.to("cpu", non_blocking=False)
+        o = d.offsets.to("cpu")
+        s = d.status.to("cpu")
+        return a, o, s
+
+    for _ in range(args.warmup):
+        step_device()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+
+    times, cell_ms, launches = [], [], 0
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            torch.cuda.synchronize(dev)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            adj, off, st = step_device()
+            e1.record()
+            torch.cuda.synchronize(dev)
+            times.append(e0.elapsed_time(e1))
+            prof = pc.last_profile()
+            cell_ms.append(prof["cells_ms"])
+            launches += int(prof["launches"])
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    total_ms = dist.reduce_max(sum(times), dev)
+    total_cells = dist.reduce_sum(float(n) * args.steps, dev)
+    value = total_cells / (total_ms / 1e3) / 1e6
+
+    # end-to-end through the public API from pinned host memory
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    e2e_times, d2h = [], 0
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        a, o, s = step_e2e()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        e2e_times.append(e0.elapsed_time(e1))
+        d2h = a.numel() * 4 + o.numel() * 4 + s.numel() * 4
+    e2e_ms = dist.reduce_max(sum(e2e_times), dev)
+    e2e_value = total_cells / (e2e_ms / 1e3) / 1e6
+    h2d = n * 12 + (n * 4 if h_w is not None else 0)
+
+    if rank == 0:
+        off_np = off.cpu().numpy()
+        flops, nbytes = algorithmic_work(off_np, spec["weighted"])
+        cell_s = statistics.mean(cell_ms) / 1e3
+        csum = clocks.summary()
+        peaks = {}
+        try:
+            peaks = json.load(open(MEASURED_PEAKS))
+        except (OSError, ValueError):
+            pass
+        peak = fp32_peak_tflops(peaks.get("sm_max_mhz") or csum.get("sm_max_mhz"))
+        achieved = flops / cell_s / 1e12 if cell_s > 0 else None
+        traffic = read_traffic_per_launch()
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                cb = cpu_oracle_rate(pts, w, args.cpu_sample)
+                cpu = {"value": cb["value"], "unit": "Mcells/s", "cores": cb["cores"], "kind": "port",
+                       "sample": f"{cb['cells']} of {n} cells; kd-tree {cb['tree_s']:.2f} s + cells "
+                                 f"{cb['cells_s']:.2f} s on {cb['cores']} threads, extrapolated to all cells"}
+            except Exception as exc:  # the baseline must not hide the GPU number
+                cpu = {"value": None, "unit": "Mcells/s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
+        line = {
+            "metric": "Mcells/s",
+            "value": value,
+            "unit": "Mcells/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": statistics.mean(times),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "n_points": n, "weighted": spec["weighted"],
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"independent diagram per GPU x{world}",
+                       "predicates": "FP32 filtered, FP64 / exact escalation"},
+            "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "kernel": "k_cells_fast (cell pass)", "cell_pass_ms": cell_s * 1e3,
+                         "algorithmic_flops": flops, "algorithmic_bytes": nbytes,
+                         "hbm_frac": (nbytes / cell_s / 1e9) / hbm_peak if cell_s > 0 else None,
+                         "peak_note": "nominal FP32 FMA peak 148 SM x 128 lanes x 2 x max SM clock "
+                                      "(MEASURED_PEAKS has no FP32 figure)"},
+            "cpu_baseline": cpu,
+            "clocks": csum,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="clustered_voronoi_5m", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-sample", type=int, default=200_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    spec = WORKLOADS[args.workload]
+    from paragram_b200 import dist
+
+    if args.impl == "reference":
+        rank, world, _ = dist.env_world()
+        run_reference(args, spec, rank, world)
+        return
+    rank, world, local = dist.init("nccl" if int(os.environ.get("WORLD_SIZE", 1)) > 1 else "gloo", timeout_s=300)
+    try:
+        run_gpu(args, spec, rank, world, local)
+    finally:
+        dist.finalize()
+
+
+if __name__ == "__main__":
+    main()

@@ -49,10 +49,9 @@ extern "C" {
  * (paragram/_api.py:65-123; defaults at paragram/csrc/ext.cpp:14-19). */
 typedef struct pg_options
 {
-    int32_t knn;        /* reference: kNN(knn) warm start (voronoi_ultra.cu:205-227). Here knn > 0
-                           enables the curve-order warm start (32 Morton neighbours); 0 disables it.
-                           Results do not depend on it. Ignored when initial guesses are given
-                           (the reference sets knn = 0 then, voronoi_ultra.cu:157-169). */
+    int32_t knn;        /* reference: kNN(knn) warm start (voronoi_ultra.cu:205-227). Accepted for
+                           compatibility: the best-first BVH traversal visits the seed's own leaf first,
+                           which serves as the warm start. Results never depend on it. */
     int32_t leaf_size;  /* reference: BVH leaf threshold, -1 = default (voronoi_ultra.cu:175-177).
                            Here <= 0 selects 16; at most 32. Results do not depend on it. */
     int32_t debug;      /* reference: print phase timings (voronoi_ultra.cu:196-219). Bit 0 prints them,

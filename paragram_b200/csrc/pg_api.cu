@@ -201,7 +201,13 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
     cl.n = n;
     cl.leaf_size = leaf;
     cl.root = n == 1 ? leaf_ref(0, 1) : (n <= leaf ? leaf_ref(0, (int)n) : 0);
-    cl.window = (guesses == nullptr && opt.knn > 0) ? kWindow : 0;
+    // The reference warm-starts every cell with its kNN(knn) (voronoi_ultra.cu:205-227). The best-first
+    // traversal here reaches the seed's own leaf first, which plays that role, so knn does not select
+    // anything; PG_WARM_WINDOW=1 adds a curve-order window warm start for experiments.
+    {
+        const char *ww = std::getenv("PG_WARM_WINDOW");
+        cl.window = (guesses == nullptr && ww && std::atoi(ww) > 0) ? kWindow : 0;
+    }
     cl.guesses = guesses;
     cl.guess_off = guess_off;
     cl.weighted = weights != nullptr;
@@ -210,6 +216,8 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
         cl.min_blocks = mb ? std::atoi(mb) : 2; // 2: warp per cell (default); 0: thread per cell
         const char *pf = std::getenv("PG_PROFILE");
         cl.prof = pf ? std::atoi(pf) : 0;
+        const char *dc = std::getenv("PG_TRACE_CELL");
+        cl.debug_cell = dc ? std::atoi(dc) : -1;
     }
     int chunks = plan_chunks(n, opt.num_chunks);
     int sms = device_sms();

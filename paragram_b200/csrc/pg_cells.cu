@@ -55,7 +55,8 @@ template <int CAP, int STACK> struct CellMem
     int pid[CAP];     // >= 0: sorted point index; < 0: -1 - box code
     unsigned vt[CAP]; // plane slots p0 | p1 << 8 | p2 << 16 (oriented)
     unsigned eb[CAP]; // boundary edges x | y << 8 of the clip in progress, by rank
-    int stk[STACK];
+    int stk[STACK];   // pending BVH references (unordered)
+    float skey[STACK]; // lower bound of the bisector distance of any point of the pending node
     unsigned long long cnt[kNumStats]; // per-warp statistics (written by lane 0)
 };
 
@@ -83,6 +84,7 @@ struct CellArgs
     int64_t big_cap;
     char *slabs;
     int prof; // accumulate per-phase clock64() cycles into the statistics
+    int debug_cell; // original index of a cell whose clips are traced with printf (-1: none)
 };
 
 enum Flag : int
@@ -497,6 +499,9 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         nb += __popc(bal);
     }
     int nv_new = count_bits(ws.valid) - count_bits(rem) + nb;
+    if (A.debug_cell == ws.soid && lane == 0)
+        printf("[pg trace] cell %d cap %d cand %d: nv %d np %d removed %d boundary %d -> nv %d\n", ws.soid, CAP, q.id,
+               count_bits(ws.valid), ws.np, count_bits(rem), nb, nv_new);
     if (nv_new > CAP)
         return kClipDefer;
     unsigned fr[W];
@@ -566,15 +571,35 @@ template <int CAP, int STACK> __device__ __forceinline__ void update_rsafe(CellM
 // Returns false when the cell is finished early (empty or deferred).
 template <int CAP, int STACK>
 __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, bool have, const Cand &q, float key,
-                          const CellArgs &A, int lane)
+                                          const CellArgs &A, int lane, const unsigned *vmask = nullptr)
 {
     // security radius: no vertex can be removed when h - eh > |a| * rsafe
     if (have && (q.h - q.eh) > q.nrm * ws.rsafe * (1.0f + 1e-6f))
         have = false;
-    if (__ballot_sync(kFull, have) == 0u)
+    unsigned hv = __ballot_sync(kFull, have);
+    if (hv == 0u)
         return true;
-    unsigned nhave = __popc(__ballot_sync(kFull, have));
-    PG_COUNT(m, lane, kStatCandidates, nhave);
+    PG_COUNT(m, lane, kStatCandidates, __popc(hv));
+    if (vmask)
+    {
+        // FP32 pre-check restricted to the vertices whose empty sphere reaches the
+        // leaf's box: a point of the leaf can remove no other vertex.
+        bool may = false;
+#pragma unroll
+        for (int k = 0; k < CAP / 32; ++k)
+        {
+            unsigned mm = vmask[k] & ws.valid[k];
+            while (mm)
+            {
+                int b = __ffs(mm) - 1;
+                mm &= mm - 1;
+                float4 X = m.vx[k * 32 + b];
+                if (have && !may)
+                    may = side_fp32(X, q) != 0;
+            }
+        }
+        have = have && may;
+    }
     unsigned todo = __ballot_sync(kFull, have);
     bool changed = false;
     while (todo)
@@ -592,6 +617,7 @@ __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP>
         if (r == kClipDefer)
         {
             ws.flags |= kFlagDefer;
+            PG_COUNT(m, lane, kStatDeferVerts, 1);
             return false;
         }
         changed = changed || r == kClipChanged;
@@ -601,33 +627,46 @@ __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP>
     return true;
 }
 
-// Can a point of this box (with max weight mw) remove a vertex of the cell?
-template <int CAP, int STACK>
-__device__ __forceinline__ bool node_may_clip(const CellMem<CAP, STACK> &m, const WarpState<CAP> &ws, float lx, float ly,
-                                              float lz, float hx, float hy, float hz, float mw, int lane, float &d2out)
+// Lower bound of the bisector distance t = (|a|^2 - dw) / (2 |a|) over the points
+// of a box (relative to the seed), and the quick security-radius rejection.
+template <int CAP>
+__device__ __forceinline__ bool box_key(const WarpState<CAP> &ws, float lx, float ly, float lz, float hx, float hy,
+                                        float hz, float mw, float &key)
 {
     float rlx = lx - ws.s.x, rly = ly - ws.s.y, rlz = lz - ws.s.z;
     float rhx = hx - ws.s.x, rhy = hy - ws.s.y, rhz = hz - ws.s.z;
     float dx = fmaxf(fmaxf(rlx, -rhx), 0.0f), dy = fmaxf(fmaxf(rly, -rhy), 0.0f), dz = fmaxf(fmaxf(rlz, -rhz), 0.0f);
     float d2 = (dx * dx + dy * dy + dz * dz) * (1.0f - 1e-6f);
-    d2out = d2;
     float dm = mw - ws.s.w;
-    float R2 = ws.rsafe * ws.rsafe * (1.0f + 1e-5f);
+    float d = sqrtf(d2) * (1.0f - 1e-6f);
+    float t;
     if (dm <= 0.0f)
-    {
-        if (d2 > 4.0f * R2)
-            return false;
-    }
+        t = 0.5f * d;
     else
     {
         float num = d2 - dm * (1.0f + 1e-6f);
-        if (num > 0.0f && num * num > 4.0f * d2 * R2)
-            return false;
+        t = (num > 0.0f && d > 0.0f) ? num / (2.0f * d) : 0.0f;
     }
+    key = t * (1.0f - 1e-5f);
+    return !(key > ws.rsafe);
+}
+
+// Vertices whose empty sphere reaches the box: q in the box can remove v only
+// if |v - q|^2 < |v - s|^2 + (w_q - w_s); per-word ballots in vm[].
+template <int CAP, int STACK>
+__device__ __forceinline__ bool node_vertex_mask(const CellMem<CAP, STACK> &m, const WarpState<CAP> &ws, float lx,
+                                                 float ly, float lz, float hx, float hy, float hz, float mw, int lane,
+                                                 unsigned *vm)
+{
+    float rlx = lx - ws.s.x, rly = ly - ws.s.y, rlz = lz - ws.s.z;
+    float rhx = hx - ws.s.x, rhy = hy - ws.s.y, rhz = hz - ws.s.z;
+    float dm = mw - ws.s.w;
     float dmu = dm > 0.0f ? dm * (1.0f + 1e-6f) : dm * (1.0f - 1e-6f);
-    bool may = false;
+    bool any = false;
 #pragma unroll
     for (int k = 0; k < CAP / 32; ++k)
+    {
+        bool may = false;
         if ((ws.valid[k] >> lane) & 1u)
         {
             int slot = k * 32 + lane;
@@ -638,10 +677,12 @@ __device__ __forceinline__ bool node_may_clip(const CellMem<CAP, STACK> &m, cons
             float ay = fmaxf(fmaxf(rly - e - X.y, X.y - rhy - e), 0.0f);
             float az = fmaxf(fmaxf(rlz - e - X.z, X.z - rhz - e), 0.0f);
             float lhs = (ax * ax + ay * ay + az * az) * (1.0f - 1e-6f);
-            if (lhs < m.vr[slot] + dmu)
-                may = true;
+            may = lhs < m.vr[slot] + dmu;
         }
-    return __ballot_sync(kFull, may) != 0u;
+        vm[k] = __ballot_sync(kFull, may);
+        any = any || vm[k] != 0u;
+    }
+    return any;
 }
 
 // Returns false when the row does not fit the fast-pass row width (the cell
@@ -747,6 +788,32 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
     return true;
 }
 
+// One BVH leaf as a candidate batch (one point per lane).
+template <int CAP, int STACK>
+__device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int ref, int i, bool guessing,
+                                           const CellArgs &A, int lane, const unsigned *vm)
+{
+    PG_COUNT(m, lane, kStatLeaves, 1);
+    int first = leaf_first(ref), count = leaf_count(ref);
+    int j = first + lane;
+    bool have = lane < count && j != i;
+    if (have && !guessing && A.window > 0 && j >= i - A.window && j <= i + A.window)
+        have = false;
+    Cand q;
+    float qkey = 0.0f;
+    if (have)
+    {
+        float4 p = A.pts[j];
+        have = !(p.x == ws.s.x && p.y == ws.s.y && p.z == ws.s.z);
+        q = make_cand(ws.s, p, j);
+        qkey = q.nrm;
+        if (guessing)
+            for (int t = 0; t < ws.np && have; ++t)
+                have = m.pid[t] != j;
+    }
+    return run_batch(m, ws, have, q, qkey, A, lane, vm);
+}
+
 template <int CAP, int STACK>
 __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int i, const CellArgs &A, int lane)
 {
@@ -808,73 +875,110 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
             return;
     }
     PG_TOC(A, m, lane, 1, tw);
-    // 2. BVH traversal, nearest child first
+    // 2. BVH traversal, best first. A pending entry is (parent << 1 | side) with
+    // a lower bound of the bisector distance of the child's points; the entry
+    // with the smallest bound is popped, dropped if the bound exceeds the radius
+    // of the (since shrunk) cell, else its box is tested against every vertex's
+    // empty sphere and, for a leaf, only the vertices that pass are pre-tested.
+    const float4 *rec = A.rec;
     int sp = 0;
-    if (lane == 0)
-        m.stk[0] = A.root;
-    sp = 1;
+    if (ref_is_leaf(A.root))
+    {
+        unsigned allv[CAP / 32];
+#pragma unroll
+        for (int k = 0; k < CAP / 32; ++k)
+            allv[k] = 0xFFFFFFFFu;
+        if (!leaf_batch(m, ws, A.root, i, guessing, A, lane, allv))
+            return;
+    }
+    else
+    {
+        if (lane == 0)
+        {
+            m.stk[0] = 0;
+            m.skey[0] = 0.0f;
+            m.stk[1] = 1;
+            m.skey[1] = 0.0f;
+        }
+        sp = 2;
+    }
     __syncwarp();
     while (sp > 0)
     {
-        int ref = m.stk[--sp];
+        unsigned best = 0xFFFFFFFFu;
+        for (int j = lane; j < sp; j += 32)
+            best = min(best, (__float_as_uint(m.skey[j]) & ~(unsigned)(STACK - 1)) | (unsigned)j);
+        best = __reduce_min_sync(kFull, best);
+        int jb = (int)(best & (unsigned)(STACK - 1));
+        int ent = m.stk[jb];
+        float key = m.skey[jb];
+        __syncwarp();
+        if (lane == 0)
+        {
+            m.stk[jb] = m.stk[sp - 1];
+            m.skey[jb] = m.skey[sp - 1];
+        }
+        --sp;
+        __syncwarp();
+        if (key > ws.rsafe)
+            continue;
+        PG_COUNT(m, lane, kStatNodes, 1);
+        PG_TIC(A, tn);
+        int parent = ent >> 1, side = ent & 1;
+        const float4 *r = rec + 4 * (size_t)parent;
+        float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+        float lx, ly, lz, hx, hy, hz, mw;
+        int ref;
+        if (side == 0)
+        {
+            lx = r0.x; ly = r0.y; lz = r0.z; hx = r0.w; hy = r1.x; hz = r1.y; mw = r3.z;
+            ref = __float_as_int(r3.x);
+        }
+        else
+        {
+            lx = r1.z; ly = r1.w; lz = r2.x; hx = r2.y; hy = r2.z; hz = r2.w; mw = r3.w;
+            ref = __float_as_int(r3.y);
+        }
+        unsigned vm[CAP / 32];
+        bool any = node_vertex_mask(m, ws, lx, ly, lz, hx, hy, hz, mw, lane, vm);
+        PG_TOC(A, m, lane, 2, tn);
+        if (!any)
+            continue;
         if (ref_is_leaf(ref))
         {
-            PG_COUNT(m, lane, kStatLeaves, 1);
-            int first = leaf_first(ref), count = leaf_count(ref);
-            int j = first + lane;
-            bool have = lane < count && j != i;
-            if (have && !guessing && A.window > 0 && j >= i - A.window && j <= i + A.window)
-                have = false;
-            Cand q;
-            float key = 0.0f;
-            if (have)
-            {
-                float4 p = A.pts[j];
-                have = !(p.x == ws.s.x && p.y == ws.s.y && p.z == ws.s.z);
-                q = make_cand(ws.s, p, j);
-                key = q.nrm;
-                if (guessing)
-                    for (int t = 0; t < ws.np && have; ++t)
-                        have = m.pid[t] != j;
-            }
             PG_TIC(A, tl);
-            bool go = run_batch(m, ws, have, q, key, A, lane);
+            bool go = leaf_batch(m, ws, ref, i, guessing, A, lane, vm);
             PG_TOC(A, m, lane, 3, tl);
             if (!go)
                 return;
             continue;
         }
-        PG_COUNT(m, lane, kStatNodes, 1);
-        PG_TIC(A, tn);
-        const float4 *r = A.rec + 4 * (size_t)ref;
-        float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
-        float d0, d1;
-        bool c0 = node_may_clip(m, ws, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r3.z, lane, d0);
-        bool c1 = node_may_clip(m, ws, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.w, lane, d1);
-        int ref0 = __float_as_int(r3.x), ref1 = __float_as_int(r3.y);
-        PG_TOC(A, m, lane, 2, tn);
+        // internal: queue both children with their distance bounds
+        const float4 *rc = rec + 4 * (size_t)ref;
+        float4 c0 = rc[0], c1 = rc[1], c2 = rc[2], c3 = rc[3];
+        float k0, k1;
+        bool p0 = box_key(ws, c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c3.z, k0);
+        bool p1 = box_key(ws, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w, c3.w, k1);
         if (sp + 2 > STACK)
         {
             ws.flags |= kFlagDefer;
+            PG_COUNT(m, lane, kStatDeferStack, 1);
             return;
         }
-        __syncwarp();
-        if (c0 && c1)
+        if (lane == 0)
         {
-            int nearr = d0 <= d1 ? ref0 : ref1, farr = d0 <= d1 ? ref1 : ref0;
-            if (lane == 0)
+            if (p0)
             {
-                m.stk[sp] = farr;
-                m.stk[sp + 1] = nearr;
+                m.stk[sp] = ref << 1;
+                m.skey[sp] = k0;
             }
-            sp += 2;
+            if (p1)
+            {
+                m.stk[sp + (p0 ? 1 : 0)] = (ref << 1) | 1;
+                m.skey[sp + (p0 ? 1 : 0)] = k1;
+            }
         }
-        else if (c0 || c1)
-        {
-            if (lane == 0)
-                m.stk[sp] = c0 ? ref0 : ref1;
-            sp += 1;
-        }
+        sp += (p0 ? 1 : 0) + (p1 ? 1 : 0);
         __syncwarp();
     }
 }
@@ -905,7 +1009,14 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
             break;
         int i = A.big_pass ? A.big_list[t] : (int)(A.begin + t);
         PG_TIC(A, tcell);
+        unsigned long long c0n = m.cnt[kStatNodes], c0l = m.cnt[kStatLeaves], c0c = m.cnt[kStatCandidates],
+                           c0k = m.cnt[kStatClips];
+        long long tbig = A.big_pass && A.debug_cell == -2 ? clock64() : 0;
         process_cell(m, ws, i, A, lane);
+        if (A.big_pass && A.debug_cell == -2 && lane == 0)
+            printf("[pg big] cell %d cycles %lld nodes %llu leaves %llu cands %llu clips %llu nv %d np %d flags %d\n",
+                   ws.soid, clock64() - tbig, m.cnt[kStatNodes] - c0n, m.cnt[kStatLeaves] - c0l,
+                   m.cnt[kStatCandidates] - c0c, m.cnt[kStatClips] - c0k, count_bits(ws.valid), ws.np, ws.flags);
         if (A.big_pass)
             ws.si = t; // the deferred-row slot
         if (ws.flags & kFlagError)
@@ -1478,6 +1589,7 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.big_cap = 0;
     A.slabs = (char *)ws.big_slabs;
     A.prof = cl.prof;
+    A.debug_cell = cl.debug_cell;
     return A;
 }
 

@@ -22,7 +22,7 @@ enum Status : int
 
 constexpr int kMaxVertsRef = 64;    // reference MAX_VERTS: more vertices => status vertex_overflow
 constexpr int kCapFast = 64;        // vertex / plane slots of a cell in shared memory
-constexpr int kStackFast = 64;      // traversal stack of a cell in shared memory
+constexpr int kStackFast = 256;     // pending BVH nodes of a cell in shared memory
 constexpr int kCapBig = 256;        // vertex / plane slots of a deferred cell (global memory)
 constexpr int kStackBig = 1024;     // traversal stack of a deferred cell
 constexpr int kRowWidth = 36;       // row slots per cell: a cell with <= 64 vertices has <= 34 faces
@@ -30,7 +30,7 @@ constexpr int kBigRowWidth = kCapBig; // row slots of a deferred cell
 constexpr int kWarpsPerBlock = 8;   // cell kernel block = 8 warps, one cell per warp at a time
 constexpr int kMaxLeaf = 32;        // leaf size limit (one candidate per lane)
 constexpr int kDefaultLeaf = 16;
-constexpr int kWindow = 16;         // warm start: sorted neighbours i-16 .. i+16
+constexpr int kWindow = 16;         // optional warm start: sorted neighbours i-16 .. i+16
 constexpr uint32_t kBigFlag = 0x40000000u; // deg[] flag: row lives in the deferred-row area
 
 // statistics counters (uint64 each) in the workspace
@@ -51,6 +51,8 @@ enum Stat : int
     kStatCycLeaves = 11, // leaf batches (pre-check + clips)
     kStatCycClips = 12,  // clips
     kStatCycOut = 13,    // row output
+    kStatDeferVerts = 14,  // deferrals / large-pass overflows: vertex or plane slots
+    kStatDeferStack = 15,  // deferrals / large-pass overflows: traversal stack
     kNumStats = 16,
 };
 

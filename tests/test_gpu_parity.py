@@ -1,0 +1,210 @@
+"""GPU parity: the CUDA builder (through the C ABI) against the CPU oracle.
+
+Bar: bit-identical sorted rows, offsets and statuses. Sizes are chosen so the
+oracle finishes in seconds; the full-size configurations are covered by
+size-independent properties (symmetry, sorted rows, no self loops, offsets).
+"""
+
+import glob
+import itertools
+import os
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def dev():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch.device("cuda:0")
+
+
+def _gpu(dev, pts, w=None, **kw):
+    import paragram_b200 as pg
+
+    t = torch.from_numpy(np.ascontiguousarray(pts)).to(dev)
+    if w is None:
+        d = pg.voronoi_diagram(t, **kw)
+    else:
+        d = pg.power_diagram(t, torch.from_numpy(np.ascontiguousarray(w)).to(dev), **kw)
+    torch.cuda.synchronize()
+    return d.adjacency.cpu().numpy(), d.offsets.cpu().numpy(), d.status.cpu().numpy()
+
+
+def _assert_same(got, exp, tag=""):
+    adj, off, st = got
+    eadj, eoff, est = exp
+    assert off.dtype == np.int32 and adj.dtype == np.int32 and st.dtype == np.int32
+    if not (np.array_equal(off, eoff) and np.array_equal(adj, eadj) and np.array_equal(st, est)):
+        bad = [i for i in range(len(st)) if st[i] != est[i] or not np.array_equal(
+            adj[off[i]:off[i + 1]] if i + 1 < len(off) else [], eadj[eoff[i]:eoff[i + 1]])]
+        raise AssertionError(f"{tag}: {len(bad)} cells differ, first {bad[:5]}")
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 17, 64, 1000, 20000])
+def test_uniform_voronoi(dev, oracle, n):
+    from paragram_b200 import workloads as W
+
+    pts = W.uniform(n, seed=n)
+    _assert_same(_gpu(dev, pts), oracle.diagram(pts), f"uniform{n}")
+
+
+def test_uniform_100k(dev, oracle):
+    from paragram_b200 import workloads as W
+
+    pts = W.uniform(100_000, seed=0)
+    _assert_same(_gpu(dev, pts), oracle.diagram(pts), "uniform100k")
+
+
+@pytest.mark.parametrize("n", [1000, 50_000])
+def test_power_uniform_with_empty_cells(dev, oracle, n):
+    from paragram_b200 import workloads as W
+
+    pts, w = W.power_uniform(n, seed=7)
+    exp = oracle.diagram(pts, w)
+    got = _gpu(dev, pts, w)
+    _assert_same(got, exp, f"power{n}")
+    if n >= 50_000:
+        assert (exp[2] == 3).sum() > 0  # the configuration has empty cells
+
+
+def test_power_heavy_weights(dev, oracle):
+    rng = np.random.default_rng(5)
+    pts = rng.random((3000, 3)).astype(np.float32)
+    w = (rng.random(3000) * 0.02).astype(np.float32)
+    _assert_same(_gpu(dev, pts, w), oracle.diagram(pts, w), "heavy")
+
+
+def test_clustered(dev, oracle):
+    from paragram_b200 import workloads as W
+
+    pts = W.clustered(100_000, seed=4)
+    _assert_same(_gpu(dev, pts), oracle.diagram(pts), "clustered100k")
+
+
+def test_surface_clouds(dev, oracle):
+    from paragram_b200 import workloads as W
+
+    for k, c in enumerate(W.surface_clouds(num_clouds=4, seed=9, size_scale=0.05)):
+        _assert_same(_gpu(dev, c), oracle.diagram(c), f"cloud{k}")
+
+
+def test_jittered_lattice_power(dev, oracle):
+    from paragram_b200 import workloads as W
+
+    pts, w = W.jittered_lattice(24, seed=1)
+    _assert_same(_gpu(dev, pts, w), oracle.diagram(pts, w), "lattice24")
+
+
+@pytest.mark.parametrize("kind", ["lattice", "duplicates", "coplanar", "collinear"])
+def test_degenerate(dev, oracle, kind):
+    rng = np.random.default_rng(11)
+    if kind == "lattice":
+        pts = np.array(list(itertools.product(np.linspace(0.1, 0.9, 6), repeat=3)), np.float32)
+    elif kind == "duplicates":
+        p = rng.random((200, 3)).astype(np.float32)
+        pts = np.concatenate([p, p[:50]])
+    elif kind == "coplanar":
+        pts = rng.random((500, 3)).astype(np.float32)
+        pts[:, 0] = 0.5
+    else:
+        pts = np.stack([np.sort(rng.random(50)), np.full(50, 0.5), np.full(50, 0.5)], 1).astype(np.float32)
+    _assert_same(_gpu(dev, pts), oracle.diagram(pts), kind)
+
+
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))))
+def test_golden_fixtures(dev, path):
+    f = np.load(path)
+    w = f["weights"] if "weights" in f.files else None
+    _assert_same(_gpu(dev, f["points"], w), (f["adjacency"], f["offsets"], f["status"]), os.path.basename(path))
+
+
+def test_results_independent_of_knobs(dev):
+    """knn, leaf_size and the chunk count are performance knobs only."""
+    import paragram_b200.cuda as pc
+    from paragram_b200 import workloads as W
+
+    pts, w = W.power_uniform(30_000, seed=2)
+    t = torch.from_numpy(pts).to(dev)
+    tw = torch.from_numpy(w).to(dev)
+    base = [x.cpu() for x in pc.build_with_stats(t, tw)[0]]
+    for kw in [dict(knn=0), dict(leaf_size=4), dict(leaf_size=32), dict(num_chunks=3), dict(knn=0, leaf_size=7)]:
+        got = [x.cpu() for x in pc.build_with_stats(t, tw, **kw)[0]]
+        assert all(torch.equal(a, b) for a, b in zip(base, got)), kw
+
+
+def test_initial_guesses_do_not_change_results(dev, oracle):
+    import paragram_b200 as pg
+    from paragram_b200 import workloads as W
+
+    pts = W.uniform(5000, seed=8)
+    exp = oracle.diagram(pts)
+    t = torch.from_numpy(pts).to(dev)
+    d = pg.voronoi_diagram(t)
+    # the true neighbours, random ids with duplicates and invalid ids, and empty lists
+    rng = np.random.default_rng(0)
+    rnd = rng.integers(-3, 5003, size=5000 * 6).astype(np.int32)
+    for guesses, offs in [(d.adjacency, d.offsets),
+                          (torch.from_numpy(rnd).to(dev), torch.arange(0, 5000 * 6 + 1, 6, dtype=torch.int32,
+                                                                       device=dev)),
+                          (torch.zeros(0, dtype=torch.int32, device=dev), torch.zeros(5001, dtype=torch.int32,
+                                                                                      device=dev))]:
+        g = pg.voronoi_diagram(t, initial_guesses=guesses, initial_guesses_offsets=offs)
+        _assert_same((g.adjacency.cpu().numpy(), g.offsets.cpu().numpy(), g.status.cpu().numpy()), exp, "guesses")
+
+
+def test_thread_per_cell_variant(dev, oracle, monkeypatch):
+    """The thread-per-cell kernel (PG_CELL_MIN_BLOCKS=0) gives the same diagram."""
+    from paragram_b200 import workloads as W
+
+    monkeypatch.setenv("PG_CELL_MIN_BLOCKS", "0")
+    pts, w = W.power_uniform(20_000, seed=21)
+    _assert_same(_gpu(dev, pts, w), oracle.diagram(pts, w), "thread-per-cell")
+
+
+def test_full_size_properties(dev):
+    """5M clustered Voronoi: symmetric, sorted, no self loops, consistent offsets."""
+    from paragram_b200 import workloads as W
+
+    pts = W.clustered(5_000_000, seed=0)
+    adj, off, st = _gpu(dev, pts)
+    n = len(pts)
+    assert off[0] == 0 and off[-1] == adj.size and (np.diff(off) >= 0).all()
+    assert set(np.unique(st).tolist()) <= {0, 2}
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(off))
+    assert (adj != rows).all()
+    # sorted rows: within a row the sequence increases
+    inc = np.diff(adj.astype(np.int64))
+    same_row = np.diff(rows) == 0
+    assert (inc[same_row] > 0).all()
+    # symmetric: the edge set equals its transpose
+    key = rows * n + adj
+    tkey = adj.astype(np.int64) * n + rows
+    assert np.array_equal(np.sort(key), np.sort(tkey))
+    deg = np.diff(off)
+    assert 14.0 < deg.mean() < 17.0
+
+
+def test_low_level_errors(dev):
+    import paragram_b200.cuda as pc
+
+    pts = torch.rand(10, 3, device=dev)
+    with pytest.raises(RuntimeError, match="weights must have 1 dimension"):
+        pc.build_laguerre_voronoi_ultra(pts, torch.rand(10, device=dev))
+    with pytest.raises(RuntimeError, match="points must be of type float"):
+        pc.build_voronoi_ultra(pts.double())
+    with pytest.raises(RuntimeError, match="leaf_size"):
+        pc.build_voronoi_ultra(pts, leaf_size=99)
+
+
+def test_empty_input(dev):
+    import paragram_b200 as pg
+
+    d = pg.voronoi_diagram(torch.zeros(0, 3, device=dev))
+    assert d.adjacency.numel() == 0 and d.offsets.tolist() == [0] and d.status.numel() == 0
