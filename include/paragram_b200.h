@@ -111,6 +111,21 @@ int pg_stats(const void *workspace, int64_t num_points, uint64_t *out, int32_t c
  * voronoi_ultra.cu:196-219, 368-373). */
 int pg_last_profile(double *out, int32_t count);
 
+/* CSR offsets from per-row degrees, allocating nothing. No counterpart in the
+ * reference: it is for callers that cannot allocate device memory when they
+ * call (a device-memory budget fixed at start-up, device memory owned by
+ * another framework's allocator, or a path that cannot afford the implicit
+ * synchronisation of cudaMalloc / cudaFree).
+ *   degrees  int32 [num_rows], non-negative, sum < 2^31 (device)
+ *   offsets  int32 [num_rows + 1] (device, output): exclusive prefix sum, offsets[num_rows] = total
+ * Its scratch is a fixed device array inside the library (129 KB per GPU,
+ * held until exit), so num_rows is limited to 2^26 - 1; larger sizes return
+ * PG_ERR_INVALID. The first call on a device resolves the array's address
+ * (cudaGetSymbolAddress) with that device current; make that first call before
+ * any stream capture. All calls on a device share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
+int pg_degrees_to_offsets_noalloc(int64_t num_rows, const int32_t *degrees, int32_t *offsets, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,7 +26,7 @@ class PgOptions(ctypes.Structure):
 
 #: Symbols declared in include/paragram_b200.h.
 EXPORTED = ["pg_version", "pg_last_error", "pg_workspace_size", "pg_build", "pg_emit_adjacency", "pg_stats",
-            "pg_last_profile"]
+            "pg_last_profile", "pg_degrees_to_offsets_noalloc"]
 
 
 def load() -> ctypes.CDLL:
@@ -55,6 +55,8 @@ def load() -> ctypes.CDLL:
         lib.pg_stats.restype = ctypes.c_int
         lib.pg_last_profile.argtypes = [ctypes.POINTER(ctypes.c_double), i32]
         lib.pg_last_profile.restype = ctypes.c_int
+        lib.pg_degrees_to_offsets_noalloc.argtypes = [i64, vp, vp, vp]
+        lib.pg_degrees_to_offsets_noalloc.restype = ctypes.c_int
         _lib = lib
         return lib
 

@@ -29,6 +29,12 @@ static int fail(int code, const std::string &msg)
     return code;
 }
 
+int set_last_error(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
 static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 static int64_t big_cap(int64_t n) { return std::min<int64_t>(n, 65536 + n / 32); }
