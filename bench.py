@@ -36,10 +36,11 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_cells_fast_clustered5m.md")
+PROFILE_SUMMARY = os.path.join(ROOT, "profiles", "k_cells_fast_clustered5m.txt")
 
 WORKLOADS = {
     "clustered_voronoi_5m": dict(kind="clustered", n=5_000_000, weighted=False),
+    "clustered_voronoi_500k": dict(kind="clustered", n=500_000, weighted=False),
     "uniform_voronoi_100k": dict(kind="uniform", n=100_000, weighted=False),
     "uniform_power_1m": dict(kind="power", n=1_000_000, weighted=True),
     "lattice_power_310": dict(kind="lattice", n=310 ** 3, weighted=True),

@@ -369,6 +369,12 @@ template <int CAP, int STACK> __device__ __forceinline__ void gc_planes(CellMem<
     __syncwarp();
 }
 
+// per-word vertex masks passed by value (an array whose address is taken lives in local memory)
+template <int W> struct VMask
+{
+    unsigned w[W];
+};
+
 enum ClipResult : int
 {
     kClipNone = 0,
@@ -571,7 +577,7 @@ template <int CAP, int STACK> __device__ __forceinline__ void update_rsafe(CellM
 // Returns false when the cell is finished early (empty or deferred).
 template <int CAP, int STACK>
 __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, bool have, const Cand &q, float key,
-                                          const CellArgs &A, int lane, const unsigned *vmask = nullptr)
+                                          const CellArgs &A, int lane, VMask<CAP / 32> vmask, bool masked)
 {
     // security radius: no vertex can be removed when h - eh > |a| * rsafe
     if (have && (q.h - q.eh) > q.nrm * ws.rsafe * (1.0f + 1e-6f))
@@ -580,7 +586,7 @@ __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP>
     if (hv == 0u)
         return true;
     PG_COUNT(m, lane, kStatCandidates, __popc(hv));
-    if (vmask)
+    if (masked)
     {
         // FP32 pre-check restricted to the vertices whose empty sphere reaches the
         // leaf's box: a point of the leaf can remove no other vertex.
@@ -588,7 +594,7 @@ __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP>
 #pragma unroll
         for (int k = 0; k < CAP / 32; ++k)
         {
-            unsigned mm = vmask[k] & ws.valid[k];
+            unsigned mm = vmask.w[k] & ws.valid[k];
             while (mm)
             {
                 int b = __ffs(mm) - 1;
@@ -656,7 +662,7 @@ __device__ __forceinline__ bool box_key(const WarpState<CAP> &ws, float lx, floa
 template <int CAP, int STACK>
 __device__ __forceinline__ bool node_vertex_mask(const CellMem<CAP, STACK> &m, const WarpState<CAP> &ws, float lx,
                                                  float ly, float lz, float hx, float hy, float hz, float mw, int lane,
-                                                 unsigned *vm)
+                                                 VMask<CAP / 32> &vm)
 {
     float rlx = lx - ws.s.x, rly = ly - ws.s.y, rlz = lz - ws.s.z;
     float rhx = hx - ws.s.x, rhy = hy - ws.s.y, rhz = hz - ws.s.z;
@@ -679,8 +685,8 @@ __device__ __forceinline__ bool node_vertex_mask(const CellMem<CAP, STACK> &m, c
             float lhs = (ax * ax + ay * ay + az * az) * (1.0f - 1e-6f);
             may = lhs < m.vr[slot] + dmu;
         }
-        vm[k] = __ballot_sync(kFull, may);
-        any = any || vm[k] != 0u;
+        vm.w[k] = __ballot_sync(kFull, may);
+        any = any || vm.w[k] != 0u;
     }
     return any;
 }
@@ -791,7 +797,7 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
 // One BVH leaf as a candidate batch (one point per lane).
 template <int CAP, int STACK>
 __device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int ref, int i, bool guessing,
-                                           const CellArgs &A, int lane, const unsigned *vm)
+                                           const CellArgs &A, int lane, VMask<CAP / 32> vm)
 {
     PG_COUNT(m, lane, kStatLeaves, 1);
     int first = leaf_first(ref), count = leaf_count(ref);
@@ -811,7 +817,7 @@ __device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP
             for (int t = 0; t < ws.np && have; ++t)
                 have = m.pid[t] != j;
     }
-    return run_batch(m, ws, have, q, qkey, A, lane, vm);
+    return run_batch(m, ws, have, q, qkey, A, lane, vm, true);
 }
 
 template <int CAP, int STACK>
@@ -853,7 +859,7 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
             unsigned peers = __match_any_sync(kFull, have ? j : -2 - lane);
             if (have && (__ffs(peers) - 1) != lane)
                 have = false;
-            if (!run_batch(m, ws, have, q, key, A, lane))
+            if (!run_batch(m, ws, have, q, key, A, lane, VMask<CAP / 32>{}, false))
                 return;
         }
     }
@@ -871,7 +877,7 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
             q = make_cand(ws.s, p, j);
             key = q.nrm;
         }
-        if (!run_batch(m, ws, have, q, key, A, lane))
+        if (!run_batch(m, ws, have, q, key, A, lane, VMask<CAP / 32>{}, false))
             return;
     }
     PG_TOC(A, m, lane, 1, tw);
@@ -884,10 +890,10 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
     int sp = 0;
     if (ref_is_leaf(A.root))
     {
-        unsigned allv[CAP / 32];
+        VMask<CAP / 32> allv;
 #pragma unroll
         for (int k = 0; k < CAP / 32; ++k)
-            allv[k] = 0xFFFFFFFFu;
+            allv.w[k] = 0xFFFFFFFFu;
         if (!leaf_batch(m, ws, A.root, i, guessing, A, lane, allv))
             return;
     }
@@ -939,7 +945,7 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
             lx = r1.z; ly = r1.w; lz = r2.x; hx = r2.y; hy = r2.z; hz = r2.w; mw = r3.w;
             ref = __float_as_int(r3.y);
         }
-        unsigned vm[CAP / 32];
+        VMask<CAP / 32> vm;
         bool any = node_vertex_mask(m, ws, lx, ly, lz, hx, hy, hz, mw, lane, vm);
         PG_TOC(A, m, lane, 2, tn);
         if (!any)
