@@ -220,10 +220,7 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
     {
         const char *mb = std::getenv("PG_CELL_MIN_BLOCKS");
         cl.min_blocks = mb ? std::atoi(mb) : 2; // 2: warp per cell (default); 0: thread per cell
-        const char *pf = std::getenv("PG_PROFILE");
-        cl.prof = pf ? std::atoi(pf) : 0;
-        const char *dc = std::getenv("PG_TRACE_CELL");
-        cl.debug_cell = dc ? std::atoi(dc) : -1;
+        cl.big_cap = big_cap(n);
     }
     int chunks = plan_chunks(n, opt.num_chunks);
     int sms = device_sms();
@@ -238,7 +235,8 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
     }
     if (timing)
         cudaEventRecord(ev[4], st);
-    cells_big_launch(ws, cl, status, big_cap(n), st);
+    if (cl.min_blocks == 0) // the thread-per-cell variant defers to a separate pass
+        cells_big_launch(ws, cl, status, big_cap(n), st);
     if (timing)
         cudaEventRecord(ev[2], st);
     csr_count(ws, n, offsets, st);

@@ -83,8 +83,7 @@ struct CellArgs
     int big_pass;
     int64_t big_cap;
     char *slabs;
-    int prof; // accumulate per-phase clock64() cycles into the statistics
-    int debug_cell; // original index of a cell whose clips are traced with printf (-1: none)
+    int inline_big; // rebuild deferred cells right away in the same kernel (warp path)
 };
 
 enum Flag : int
@@ -114,10 +113,7 @@ template <int CAP> struct WarpState
         if ((lane) == 0)                                                                                               \
             (m).cnt[idx] += pg_count_v_;                                                                               \
     } while (0)
-#define PG_TIC(A, v) long long v = (A).prof ? clock64() : 0
-#define PG_TOC(A, m, lane, slot, v)                                                                                    \
-    if ((A).prof && (lane) == 0)                                                                                       \
-    (m).cnt[kStatCycCell + (slot)] += (unsigned long long)(clock64() - v)
+
 
 struct Cand
 {
@@ -138,7 +134,7 @@ __device__ __forceinline__ Cand make_cand(float4 s, float4 q, int id)
     float dw = q.w - s.w;
     c.h = 0.5f * __fsub_rn(n2, dw);
     c.eh = 2.0f * kEps * (fabsf(c.h) + 3.0f * n2 + fabsf(dw));
-    c.nrm = __fsqrt_rn(n2) * (1.0f + 8.0f * kEps);
+    c.nrm = n2 * rsqrtf(n2) * (1.0f + 4e-6f); // rsqrtf: <= 2 ulp
     c.cerr = (3.0f * kEps * fabsf(c.h) + c.eh) * (1.0f + 8.0f * kEps);
     if (!(n2 > 1e-30f && n2 < 1e30f))
         c.cerr = INFINITY; // out of the filter's range: always exact
@@ -217,20 +213,24 @@ __device__ __forceinline__ float4 make_vertex(float4 a, float ea, float4 b, floa
     float nx = a.w * u0x + b.w * u1x + c.w * u2x;
     float ny = a.w * u0y + b.w * u1y + c.w * u2y;
     float nz = a.w * u0z + b.w * u1z + c.w * u2z;
-    float X = __fdiv_rn(nx, D), Y = __fdiv_rn(ny, D), Z = __fdiv_rn(nz, D);
-    float xn = __fsqrt_rn(X * X + Y * Y + Z * Z);
+    // any FP32 point is acceptable here: the bound below is a-posteriori
+    float rD = __frcp_rn(D);
+    float X = nx * rD, Y = ny * rD, Z = nz * rD;
+    float x2 = X * X + Y * Y + Z * Z;
+    float xn = x2 > 0.0f ? x2 * rsqrtf(x2) * (1.0f + 4e-6f) : 0.0f;
     float la = fabsf(a.x) + fabsf(a.y) + fabsf(a.z);
     float lb = fabsf(b.x) + fabsf(b.y) + fabsf(b.z);
     float lc = fabsf(c.x) + fabsf(c.y) + fabsf(c.z);
     float ra = fabsf(__fmaf_rn(a.x, X, __fmaf_rn(a.y, Y, __fmaf_rn(a.z, Z, -a.w)))) + 4.0f * kEps * (la * xn + fabsf(a.w)) + ea;
     float rb = fabsf(__fmaf_rn(b.x, X, __fmaf_rn(b.y, Y, __fmaf_rn(b.z, Z, -b.w)))) + 4.0f * kEps * (lb * xn + fabsf(b.w)) + eb;
     float rc = fabsf(__fmaf_rn(c.x, X, __fmaf_rn(c.y, Y, __fmaf_rn(c.z, Z, -c.w)))) + 4.0f * kEps * (lc * xn + fabsf(c.w)) + ec;
-    float rho = sqrtf(ra * ra + rb * rb + rc * rc);
-    float F = sqrtf(u0x * u0x + u0y * u0y + u0z * u0z + u1x * u1x + u1y * u1y + u1z * u1z + u2x * u2x + u2y * u2y +
-                    u2z * u2z) +
-              8.0f * kEps * (lb * lc + lc * la + la * lb);
+    float r2 = ra * ra + rb * rb + rc * rc;
+    float rho = r2 > 0.0f ? r2 * rsqrtf(r2) * (1.0f + 4e-6f) : 0.0f;
+    float f2 = u0x * u0x + u0y * u0y + u0z * u0z + u1x * u1x + u1y * u1y + u1z * u1z + u2x * u2x + u2y * u2y +
+               u2z * u2z;
+    float F = (f2 > 0.0f ? f2 * rsqrtf(f2) * (1.0f + 4e-6f) : 0.0f) + 8.0f * kEps * (lb * lc + lc * la + la * lb);
     float den = fabsf(D) - 8.0f * kEps * la * lb * lc;
-    float ex = den > 0.0f ? F * rho / den : INFINITY;
+    float ex = den > 0.0f ? __fdividef(F * rho, den) * (1.0f + 4e-6f) : INFINITY;
     float psi = (2.0f * ex + 4.0f * kEps * xn) * (1.0f + 1e-6f);
     if (!(psi < 1e30f) || !(xn < 1e30f))
         psi = INFINITY;
@@ -505,9 +505,6 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         nb += __popc(bal);
     }
     int nv_new = count_bits(ws.valid) - count_bits(rem) + nb;
-    if (A.debug_cell == ws.soid && lane == 0)
-        printf("[pg trace] cell %d cap %d cand %d: nv %d np %d removed %d boundary %d -> nv %d\n", ws.soid, CAP, q.id,
-               count_bits(ws.valid), ws.np, count_bits(rem), nb, nv_new);
     if (nv_new > CAP)
         return kClipDefer;
     unsigned fr[W];
@@ -615,9 +612,7 @@ __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP>
         int src = (int)(mn & 31u);
         todo &= ~(1u << src);
         Cand c = shfl_cand(q, src);
-        PG_TIC(A, tc);
         int r = clip(m, ws, c, A, lane);
-        PG_TOC(A, m, lane, 4, tc);
         if (r == kClipEmptied)
             return false;
         if (r == kClipDefer)
@@ -644,14 +639,14 @@ __device__ __forceinline__ bool box_key(const WarpState<CAP> &ws, float lx, floa
     float dx = fmaxf(fmaxf(rlx, -rhx), 0.0f), dy = fmaxf(fmaxf(rly, -rhy), 0.0f), dz = fmaxf(fmaxf(rlz, -rhz), 0.0f);
     float d2 = (dx * dx + dy * dy + dz * dz) * (1.0f - 1e-6f);
     float dm = mw - ws.s.w;
-    float d = sqrtf(d2) * (1.0f - 1e-6f);
+    float d = d2 > 0.0f ? d2 * rsqrtf(d2) * (1.0f - 4e-6f) : 0.0f; // lower bound of the box distance
     float t;
     if (dm <= 0.0f)
         t = 0.5f * d;
     else
     {
         float num = d2 - dm * (1.0f + 1e-6f);
-        t = (num > 0.0f && d > 0.0f) ? num / (2.0f * d) : 0.0f;
+        t = (num > 0.0f && d > 0.0f) ? __fdividef(num, 2.0f * d) * (1.0f - 4e-6f) : 0.0f;
     }
     key = t * (1.0f - 1e-5f);
     return !(key > ws.rsafe);
@@ -694,7 +689,8 @@ __device__ __forceinline__ bool node_vertex_mask(const CellMem<CAP, STACK> &m, c
 // Returns false when the row does not fit the fast-pass row width (the cell
 // is then deferred to the large-capacity pass).
 template <int CAP, int STACK>
-__device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, const CellArgs &A, int lane)
+__device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, const CellArgs &A, int lane,
+                                              bool big)
 {
     constexpr int W = CAP / 32;
     int oi = ws.soid;
@@ -762,14 +758,14 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
                 rnk[kk] += (v < o[kk]);
         }
     }
-    if (!A.big_pass && cnt > kRowWidth)
+    if (!big && cnt > kRowWidth)
         return false;
     int nverts = count_bits(ws.valid);
     int st = nverts > kMaxVertsRef ? kVertexOverflow : kSuccess;
     if (ws.flags & kFlagDefer)
         st = kPlaneOverflow; // only reachable in the large-capacity pass
     int *row;
-    if (A.big_pass)
+    if (big)
     {
         int bi = ws.si; // index in the deferred list
         row = A.big_rows + (size_t)bi * kBigRowWidth;
@@ -795,15 +791,15 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
 }
 
 // One BVH leaf as a candidate batch (one point per lane).
-template <int CAP, int STACK>
-__device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int ref, int i, bool guessing,
+template <int CAP, int STACK, bool GUESS>
+__device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int ref, int i,
                                            const CellArgs &A, int lane, VMask<CAP / 32> vm)
 {
     PG_COUNT(m, lane, kStatLeaves, 1);
     int first = leaf_first(ref), count = leaf_count(ref);
     int j = first + lane;
     bool have = lane < count && j != i;
-    if (have && !guessing && A.window > 0 && j >= i - A.window && j <= i + A.window)
+    if (have && !GUESS && A.window > 0 && j >= i - A.window && j <= i + A.window)
         have = false;
     Cand q;
     float qkey = 0.0f;
@@ -813,14 +809,14 @@ __device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP
         have = !(p.x == ws.s.x && p.y == ws.s.y && p.z == ws.s.z);
         q = make_cand(ws.s, p, j);
         qkey = q.nrm;
-        if (guessing)
+        if (GUESS)
             for (int t = 0; t < ws.np && have; ++t)
                 have = m.pid[t] != j;
     }
     return run_batch(m, ws, have, q, qkey, A, lane, vm, true);
 }
 
-template <int CAP, int STACK>
+template <int CAP, int STACK, bool GUESS>
 __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int i, const CellArgs &A, int lane)
 {
     ws.s = A.pts[i];
@@ -828,8 +824,7 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
     ws.soid = A.oid[i];
     cell_init(m, ws, A, lane);
     const int n = A.n;
-    const bool guessing = A.guesses != nullptr;
-    PG_TIC(A, tw);
+    const bool guessing = GUESS;
     // 1. warm start: curve-order neighbours (or the caller's initial guesses)
     if (guessing)
     {
@@ -880,7 +875,6 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
         if (!run_batch(m, ws, have, q, key, A, lane, VMask<CAP / 32>{}, false))
             return;
     }
-    PG_TOC(A, m, lane, 1, tw);
     // 2. BVH traversal, best first. A pending entry is (parent << 1 | side) with
     // a lower bound of the bisector distance of the child's points; the entry
     // with the smallest bound is popped, dropped if the bound exceeds the radius
@@ -894,7 +888,7 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
 #pragma unroll
         for (int k = 0; k < CAP / 32; ++k)
             allv.w[k] = 0xFFFFFFFFu;
-        if (!leaf_batch(m, ws, A.root, i, guessing, A, lane, allv))
+        if (!leaf_batch<CAP, STACK, GUESS>(m, ws, A.root, i, A, lane, allv))
             return;
     }
     else
@@ -929,7 +923,6 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
         if (key > ws.rsafe)
             continue;
         PG_COUNT(m, lane, kStatNodes, 1);
-        PG_TIC(A, tn);
         int parent = ent >> 1, side = ent & 1;
         const float4 *r = rec + 4 * (size_t)parent;
         float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
@@ -947,14 +940,11 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
         }
         VMask<CAP / 32> vm;
         bool any = node_vertex_mask(m, ws, lx, ly, lz, hx, hy, hz, mw, lane, vm);
-        PG_TOC(A, m, lane, 2, tn);
         if (!any)
             continue;
         if (ref_is_leaf(ref))
         {
-            PG_TIC(A, tl);
-            bool go = leaf_batch(m, ws, ref, i, guessing, A, lane, vm);
-            PG_TOC(A, m, lane, 3, tl);
+            bool go = leaf_batch<CAP, STACK, GUESS>(m, ws, ref, i, A, lane, vm);
             if (!go)
                 return;
             continue;
@@ -996,7 +986,40 @@ template <int CAP, int STACK> __device__ void flush_stats(CellMem<CAP, STACK> &m
         atomicAdd(&A.stats[lane], m.cnt[lane]);
 }
 
-template <int CAP, int STACK>
+// Rebuild cell i with 256 vertex / plane slots and a 1024-entry queue in this
+// warp's global slab. Called by the warp whose shared-memory cell outgrew its
+// 64 slots, right away, so that the few expensive cells overlap with the rest
+// of the cell pass instead of forming a tail after it.
+template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, int i, int lane)
+{
+    size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    auto &m = *reinterpret_cast<CellMem<kCapBig, kStackBig> *>(A.slabs + gw * sizeof(CellMem<kCapBig, kStackBig>));
+    WarpState<kCapBig> ws;
+    if (lane < kNumStats)
+        m.cnt[lane] = 0;
+    int slot = 0;
+    if (lane == 0)
+        slot = atomicAdd(&A.counters[1], 1);
+    slot = __shfl_sync(kFull, slot, 0);
+    __syncwarp();
+    process_cell<kCapBig, kStackBig, GUESS>(m, ws, i, A, lane);
+    if ((ws.flags & kFlagError) && lane == 0)
+        atomicExch(&A.counters[2], 1);
+    if (slot < A.big_cap)
+    {
+        ws.si = slot; // deferred-row slot
+        write_outputs(m, ws, A, lane, true);
+    }
+    else if (lane == 0)
+    {
+        // out of deferred-row slots: reported by the host as an error
+        A.deg[ws.soid] = 0;
+        A.status[ws.soid] = kPlaneOverflow;
+    }
+    flush_stats(m, A, lane);
+}
+
+template <int CAP, int STACK, bool GUESS>
 __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArgs &A, int lane)
 {
     WarpState<CAP> ws;
@@ -1014,15 +1037,7 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
         if (t >= count)
             break;
         int i = A.big_pass ? A.big_list[t] : (int)(A.begin + t);
-        PG_TIC(A, tcell);
-        unsigned long long c0n = m.cnt[kStatNodes], c0l = m.cnt[kStatLeaves], c0c = m.cnt[kStatCandidates],
-                           c0k = m.cnt[kStatClips];
-        long long tbig = A.big_pass && A.debug_cell == -2 ? clock64() : 0;
-        process_cell(m, ws, i, A, lane);
-        if (A.big_pass && A.debug_cell == -2 && lane == 0)
-            printf("[pg big] cell %d cycles %lld nodes %llu leaves %llu cands %llu clips %llu nv %d np %d flags %d\n",
-                   ws.soid, clock64() - tbig, m.cnt[kStatNodes] - c0n, m.cnt[kStatLeaves] - c0l,
-                   m.cnt[kStatCandidates] - c0c, m.cnt[kStatClips] - c0k, count_bits(ws.valid), ws.np, ws.flags);
+        process_cell<CAP, STACK, GUESS>(m, ws, i, A, lane);
         if (A.big_pass)
             ws.si = t; // the deferred-row slot
         if (ws.flags & kFlagError)
@@ -1032,13 +1047,13 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
             ws.flags &= ~kFlagError;
         }
         if (!(ws.flags & kFlagDefer) || A.big_pass)
-        {
-            PG_TIC(A, to);
-            bool ok = write_outputs(m, ws, A, lane);
-            PG_TOC(A, m, lane, 5, to);
-            PG_TOC(A, m, lane, 0, tcell);
-            if (ok)
+            if (write_outputs(m, ws, A, lane, A.big_pass != 0))
                 continue;
+        PG_COUNT(m, lane, kStatDeferred, 1);
+        if (A.inline_big)
+        {
+            big_cell<GUESS>(A, i, lane);
+            continue;
         }
         // deferred: placeholder outputs (an empty row) until the large-capacity pass
         if (lane == 0)
@@ -1047,25 +1062,25 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
             A.status[ws.soid] = kPlaneOverflow;
             int d = atomicAdd(&A.counters[1], 1);
             A.big_list[d] = i;
-            atomicAdd(&A.stats[kStatDeferred], 1ull);
         }
     }
     flush_stats(m, A, lane);
 }
 
-template <int MINB> __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) k_cells_fast(CellArgs A)
+template <int MINB, bool GUESS>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) k_cells_fast(CellArgs A)
 {
     __shared__ CellMem<kCapFast, kStackFast> mem[kWarpsPerBlock];
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    cells_body(mem[w], A, lane);
+    cells_body<kCapFast, kStackFast, GUESS>(mem[w], A, lane);
 }
 
-__global__ void __launch_bounds__(kWarpsPerBlock * 32) k_cells_big(CellArgs A)
+template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_cells_big(CellArgs A)
 {
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     size_t gw = (size_t)blockIdx.x * kWarpsPerBlock + w;
     auto *m = reinterpret_cast<CellMem<kCapBig, kStackBig> *>(A.slabs + gw * sizeof(CellMem<kCapBig, kStackBig>));
-    cells_body(*m, A, lane);
+    cells_body<kCapBig, kStackBig, GUESS>(*m, A, lane);
 }
 
 // ===========================================================================
@@ -1566,7 +1581,7 @@ __global__ void __launch_bounds__(256, 4) k_tcells(CellArgs A, TSlab *slabs)
 int tcell_threads() { return 148 * 1024; }
 size_t tcell_slab_bytes() { return sizeof(TSlab) * (size_t)(tcell_threads() / 32); }
 
-int big_warps() { return 148 * kWarpsPerBlock; }
+int big_warps() { return 148 * 4 * kWarpsPerBlock; } // one slab per resident warp (<= 4 blocks / SM)
 size_t big_slab_bytes() { return sizeof(CellMem<kCapBig, kStackBig>) * (size_t)big_warps(); }
 
 static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
@@ -1594,8 +1609,7 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.big_pass = 0;
     A.big_cap = 0;
     A.slabs = (char *)ws.big_slabs;
-    A.prof = cl.prof;
-    A.debug_cell = cl.debug_cell;
+    A.inline_big = 0;
     return A;
 }
 
@@ -1620,12 +1634,15 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
         k_tcells<<<(unsigned)grid, 256, 0, st>>>(A, (TSlab *)ws.tslabs);
         return;
     }
-    void (*kern)(CellArgs) = k_cells_fast<2>;
+    void (*kern)(CellArgs) = cl.guesses ? k_cells_fast<2, true>
+                                        : (cl.min_blocks == 3 ? k_cells_fast<3, false> : k_cells_fast<2, false>);
     int blocks_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerBlock * 32, 0);
     if (blocks_per_sm < 1)
         blocks_per_sm = 1;
-    int64_t grid = (int64_t)num_sms * blocks_per_sm;
+    A.inline_big = 1;
+    A.big_cap = cl.big_cap;
+    int64_t grid = std::min<int64_t>((int64_t)num_sms * blocks_per_sm, big_warps() / kWarpsPerBlock);
     int64_t need = (cells + kWarpsPerBlock - 1) / kWarpsPerBlock;
     if (grid > need)
         grid = need;
@@ -1643,7 +1660,10 @@ void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, in
     A.big_pass = 1;
     A.big_cap = big_cap;
     ++g_launches;
-    k_cells_big<<<(unsigned)(big_warps() / kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(A);
+    if (cl.guesses)
+        k_cells_big<true><<<(unsigned)(big_warps() / kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(A);
+    else
+        k_cells_big<false><<<(unsigned)(big_warps() / kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(A);
 }
 
 } // namespace pg

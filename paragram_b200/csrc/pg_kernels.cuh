@@ -30,8 +30,7 @@ struct CellLaunch
     int64_t cell_begin, cell_end; // sorted-slot range of this launch
     int weighted;
     int min_blocks; // register-budget variant of the cell kernel (2, 3 or 4 blocks per SM)
-    int prof;       // per-phase cycle counters
-    int debug_cell; // original index of a cell traced with printf, -1 for none
+    int64_t big_cap; // deferred-row slots
 };
 void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int num_sms, cudaStream_t st);
 void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st);
