@@ -59,6 +59,9 @@ typedef struct pg_options
     int32_t num_chunks; /* reference: PARAGRAM_NUM_CHUNKS / PARAGRAM_MEM_FRAC chunk plan
                            (chunking.h:16-56). 0 = read the environment; > 0 = split the cell
                            pass into this many launches. Results do not depend on it. */
+    int32_t blocks_per_sm; /* register budget of the cell kernel: resident blocks of 8 warps per SM
+                              (2 or 3; 0 = default 2). No reference counterpart; chosen by the
+                              autotuner. Results do not depend on it. */
 } pg_options;
 
 /* Library version (major * 10000 + minor * 100 + patch). */
@@ -79,7 +82,7 @@ int pg_workspace_size(int64_t num_points, size_t *bytes);
  *   initial_guesses / initial_guesses_offsets
  *               int32 CSR of candidate neighbours per point (original ids), or both NULL
  *               (reference: voronoi_ultra.cu:69-85). Results do not depend on them.
- *   options     host pointer or NULL (defaults: knn 8, leaf_size -1, debug 0, num_chunks 0)
+ *   options     host pointer or NULL (defaults: knn 8, leaf_size -1, debug 0, num_chunks 0, blocks_per_sm 0)
  *   workspace   device buffer of at least pg_workspace_size() bytes, 256-byte aligned;
  *               it must stay alive until pg_emit_adjacency returns
  *   offsets     int32 [num_points + 1]  (output)
@@ -110,6 +113,23 @@ int pg_stats(const void *workspace, int64_t num_points, uint64_t *out, int32_t c
  * No reference counterpart (the reference prints timings with debug=True,
  * voronoi_ultra.cu:196-219, 368-373). */
 int pg_last_profile(double *out, int32_t count);
+
+/* ---- Batches: many independent point clouds in one build --------------------
+ * No single reference counterpart: the reference builds one cloud per call
+ * (paragram/_api.py:65-123); a batch is equivalent to one call per cloud.
+ * Cloud c owns points [cloud_offsets[c], cloud_offsets[c+1]) of the concatenated
+ * arrays; every cloud gets its own box and its own diagram. Output: one CSR over
+ * all points whose rows list GLOBAL point indices (a cloud's rows only list its
+ * own points); offsets [total + 1], status [total].
+ * With num_edges == NULL the call never synchronises: the total edge count stays
+ * in offsets[total] on the device, the whole call can be captured in a CUDA graph,
+ * and pg_batch_check reports errors afterwards. pg_emit_adjacency fills the
+ * adjacency as for a single diagram. */
+int pg_batch_workspace_size(int64_t total_points, int32_t num_clouds, size_t *bytes);
+int pg_build_batch(int64_t total_points, int32_t num_clouds, const int32_t *cloud_offsets, const float *points,
+                   const float *weights, const pg_options *options, void *workspace, size_t workspace_bytes,
+                   int32_t *offsets, int32_t *status, int64_t *num_edges, void *stream);
+int pg_batch_check(const void *workspace, int64_t total_points, int32_t num_clouds, void *stream);
 
 /* CSR offsets from per-row degrees, allocating nothing. No counterpart in the
  * reference: it is for callers that cannot allocate device memory when they

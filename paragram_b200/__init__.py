@@ -7,9 +7,11 @@ fallback -- calling the API without the built library raises ImportError.
 """
 
 from ._api import Diagram, power_diagram, voronoi_diagram
+from .batch import build_batch
 
 __all__ = [
     "Diagram",
+    "build_batch",
     "power_diagram",
     "voronoi_diagram",
 ]

@@ -21,12 +21,14 @@ class PgOptions(ctypes.Structure):
         ("leaf_size", ctypes.c_int32),
         ("debug", ctypes.c_int32),
         ("num_chunks", ctypes.c_int32),
+        ("blocks_per_sm", ctypes.c_int32),
     ]
 
 
 #: Symbols declared in include/paragram_b200.h.
 EXPORTED = ["pg_version", "pg_last_error", "pg_workspace_size", "pg_build", "pg_emit_adjacency", "pg_stats",
-            "pg_last_profile", "pg_degrees_to_offsets_noalloc"]
+            "pg_last_profile", "pg_degrees_to_offsets_noalloc", "pg_batch_workspace_size", "pg_build_batch",
+            "pg_batch_check"]
 
 
 def load() -> ctypes.CDLL:
@@ -55,6 +57,13 @@ def load() -> ctypes.CDLL:
         lib.pg_stats.restype = ctypes.c_int
         lib.pg_last_profile.argtypes = [ctypes.POINTER(ctypes.c_double), i32]
         lib.pg_last_profile.restype = ctypes.c_int
+        lib.pg_batch_workspace_size.argtypes = [i64, i32, ctypes.POINTER(sz)]
+        lib.pg_batch_workspace_size.restype = ctypes.c_int
+        lib.pg_build_batch.argtypes = [i64, i32, vp, vp, vp, ctypes.POINTER(PgOptions), vp, sz, vp, vp,
+                                       ctypes.POINTER(i64), vp]
+        lib.pg_build_batch.restype = ctypes.c_int
+        lib.pg_batch_check.argtypes = [vp, i64, i32, vp]
+        lib.pg_batch_check.restype = ctypes.c_int
         lib.pg_degrees_to_offsets_noalloc.argtypes = [i64, vp, vp, vp]
         lib.pg_degrees_to_offsets_noalloc.restype = ctypes.c_int
         _lib = lib

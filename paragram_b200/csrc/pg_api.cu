@@ -39,8 +39,9 @@ static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 static int64_t big_cap(int64_t n) { return std::min<int64_t>(n, 65536 + n / 32); }
 
-size_t workspace_layout(int64_t n, char *base, Workspace *ws)
+size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
 {
+    size_t C = (size_t)std::max(num_clouds, 1);
     size_t off = 0;
     auto take = [&](size_t bytes) -> char * {
         char *p = base ? base + off : nullptr;
@@ -52,9 +53,6 @@ size_t workspace_layout(int64_t n, char *base, Workspace *ws)
     size_t hist_elems = (size_t)256 * blocks + 1;
     size_t scan_elems = scan_tmp_elems((int64_t)std::max(hist_elems, N + 1));
     Workspace w;
-    w.bounds = (int *)take(8 * sizeof(int));
-    w.box = (float *)take(8 * sizeof(float));
-    w.morton = (float *)take(4 * sizeof(float));
     w.counters = (int *)take(16 * sizeof(int));
     w.stats = (unsigned long long *)take(kNumStats * sizeof(unsigned long long));
     w.keys0 = (unsigned long long *)take(8 * N);
@@ -85,6 +83,12 @@ size_t workspace_layout(int64_t n, char *base, Workspace *ws)
     w.miss = (int *)take(4 * N);
     w.fill = (int *)take(4 * N);
     w.sizes = (uint32_t *)take(4 * (N + 1));
+    // per-cloud segments last, so that every other offset is independent of the cloud count
+    w.bounds = (int *)take(8 * C * sizeof(int));
+    w.box = (float *)take(8 * C * sizeof(float));
+    w.morton = (float *)take(4 * C * sizeof(float));
+    w.cloud_off = (int *)take((C + 1) * sizeof(int));
+    w.cloud_root = (int *)take(C * sizeof(int));
     w.bytes = off;
     if (ws)
         *ws = w;
@@ -133,38 +137,43 @@ static int device_sms()
     return sms;
 }
 
-} // namespace pg
 
-extern "C" {
-
-int pg_version(void) { return 100; }
-
-const char *pg_last_error(void) { return pg::g_last_error.c_str(); }
-
-int pg_workspace_size(int64_t num_points, size_t *bytes)
+__global__ void k_single_cloud(int *off, int n)
 {
-    if (!bytes)
-        return pg::fail(PG_ERR_INVALID, "bytes must not be NULL");
-    if (num_points < 0 || num_points >= pg::kMaxPoints)
-        return pg::fail(PG_ERR_INVALID, "num_points must be in [0, 2^26)");
-    *bytes = pg::workspace_layout(num_points, nullptr, nullptr);
+    off[0] = 0;
+    off[1] = n;
+}
+
+static int check_counters(const int *host, int64_t n)
+{
+    if (host[2] == 1)
+        return fail(PG_ERR_INTERNAL, "exact predicate exceeded its expansion capacity");
+    if (host[2] == 2)
+        return fail(PG_ERR_INTERNAL, "a cloud's points do not form one BVH subtree");
+    if (host[1] > big_cap(n))
+        return fail(PG_ERR_INTERNAL, "too many cells exceeded 64 vertices (" + std::to_string(host[1]) +
+                                         " > capacity " + std::to_string(big_cap(n)) + ")");
     return PG_OK;
 }
 
-int pg_build(int64_t n, const float *points, const float *weights, const int32_t *guesses, const int32_t *guess_off,
-             const pg_options *options, void *workspace, size_t workspace_bytes, int32_t *offsets, int32_t *status,
-             int64_t *num_edges, void *stream)
+// One build of num_clouds independent diagrams over n points (cloud c owns points
+// [cloud_offsets[c], cloud_offsets[c+1]) ). num_edges == NULL: no host synchronisation
+// (the total stays in offsets[n] on the device; errors via pg_batch_check).
+static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, const float *points,
+                      const float *weights, const int32_t *guesses, const int32_t *guess_off,
+                      const pg_options *options, void *workspace, size_t workspace_bytes, int32_t *offsets,
+                      int32_t *status, int64_t *num_edges, void *stream)
 {
-    using namespace pg;
     g_last_error.clear();
     cudaStream_t st = (cudaStream_t)stream;
-    pg_options opt = {8, -1, 0, 0};
+    pg_options opt = {8, -1, 0, 0, 0};
     if (options)
         opt = *options;
+    const bool sync = num_edges != nullptr;
     if (n < 0 || n >= kMaxPoints)
         return fail(PG_ERR_INVALID, "num_points must be in [0, 2^26)");
-    if (!num_edges || !offsets)
-        return fail(PG_ERR_INVALID, "offsets and num_edges must not be NULL");
+    if (!offsets)
+        return fail(PG_ERR_INVALID, "offsets must not be NULL");
     if ((guesses == nullptr) != (guess_off == nullptr))
         return fail(PG_ERR_INVALID, "initial_guesses and initial_guesses_offsets must be provided together");
     if (n > 0 && (!points || !status || !workspace))
@@ -173,25 +182,27 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
         return fail(PG_ERR_INVALID, "workspace must be 256-byte aligned");
     if (opt.leaf_size > kMaxLeaf)
         return fail(PG_ERR_INVALID, "leaf_size must be at most 32");
-    size_t need = workspace_layout(n, nullptr, nullptr);
+    size_t need = workspace_layout(n, num_clouds, nullptr, nullptr);
     if (workspace_bytes < need)
         return fail(PG_ERR_INVALID, "workspace too small: need " + std::to_string(need) + " bytes");
     cudaGetLastError();
     if (n == 0)
     {
         cudaMemsetAsync(offsets, 0, sizeof(int32_t), st);
+        if (!sync)
+            return PG_OK;
         *num_edges = 0;
         cudaError_t e = cudaStreamSynchronize(st);
         return e == cudaSuccess ? PG_OK : fail(PG_ERR_CUDA, cudaGetErrorString(e));
     }
     Workspace ws;
-    workspace_layout(n, (char *)workspace, &ws);
+    workspace_layout(n, num_clouds, (char *)workspace, &ws);
     int leaf = opt.leaf_size > 0 ? opt.leaf_size : kDefaultLeaf;
     g_launches = 0;
     for (double &v : g_profile)
         v = 0.0;
     // debug bit 0: print phase timings (reference behaviour); bit 1: record them for pg_last_profile
-    const bool timing = opt.debug != 0;
+    const bool timing = sync && opt.debug != 0;
     cudaEvent_t ev[5];
     if (timing)
         for (auto &e : ev)
@@ -200,13 +211,21 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
         cudaEventRecord(ev[0], st);
     cudaMemsetAsync(ws.counters, 0, 16 * sizeof(int), st);
     cudaMemsetAsync(ws.stats, 0, kNumStats * sizeof(unsigned long long), st);
-    lbvh_build(ws, n, points, weights, leaf, st);
+    if (cloud_offsets)
+        cudaMemcpyAsync(ws.cloud_off, cloud_offsets, sizeof(int) * (size_t)(num_clouds + 1), cudaMemcpyDeviceToDevice,
+                        st);
+    else
+    {
+        ++g_launches;
+        k_single_cloud<<<1, 1, 0, st>>>(ws.cloud_off, (int)n);
+    }
+    lbvh_build(ws, n, num_clouds, points, weights, leaf, st);
     if (timing)
         cudaEventRecord(ev[1], st);
     CellLaunch cl;
     cl.n = n;
     cl.leaf_size = leaf;
-    cl.root = n == 1 ? leaf_ref(0, 1) : (n <= leaf ? leaf_ref(0, (int)n) : 0);
+    cl.num_clouds = num_clouds;
     // The reference warm-starts every cell with its kNN(knn) (voronoi_ultra.cu:205-227). The best-first
     // traversal here reaches the seed's own leaf first, which plays that role, so knn does not select
     // anything; PG_WARM_WINDOW=1 adds a curve-order window warm start for experiments.
@@ -218,11 +237,12 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
     cl.guess_off = guess_off;
     cl.weighted = weights != nullptr;
     {
+        // warp per cell with 2 (default) or 3 blocks per SM; PG_CELL_MIN_BLOCKS=0 selects thread per cell
         const char *mb = std::getenv("PG_CELL_MIN_BLOCKS");
-        cl.min_blocks = mb ? std::atoi(mb) : 2; // 2: warp per cell (default); 0: thread per cell
+        cl.min_blocks = mb ? std::atoi(mb) : (opt.blocks_per_sm == 3 ? 3 : 2);
         cl.big_cap = big_cap(n);
     }
-    int chunks = plan_chunks(n, opt.num_chunks);
+    int chunks = sync ? plan_chunks(n, opt.num_chunks) : std::max(opt.num_chunks, 1);
     int sms = device_sms();
     int64_t per = (n + chunks - 1) / chunks;
     for (int c = 0; c < chunks; ++c)
@@ -240,6 +260,13 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
     if (timing)
         cudaEventRecord(ev[2], st);
     csr_count(ws, n, offsets, st);
+    g_profile[0] = (double)g_launches;
+    g_profile[6] = (double)chunks;
+    if (!sync)
+    {
+        cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? PG_OK : fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    }
     int host[4] = {0, 0, 0, 0};
     int64_t edges = 0;
     {
@@ -274,19 +301,77 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
         for (auto &e : ev)
             cudaEventDestroy(e);
     }
-    g_profile[0] = (double)g_launches;
     g_profile[5] = (double)host[1];
-    g_profile[6] = (double)chunks;
-    if (host[2] != 0)
-        return fail(PG_ERR_INTERNAL, "exact predicate exceeded its expansion capacity");
-    if (host[1] > big_cap(n))
-        return fail(PG_ERR_INTERNAL, "too many cells exceeded 64 vertices (" + std::to_string(host[1]) +
-                                         " > capacity " + std::to_string(big_cap(n)) + ")");
+    int rc = check_counters(host, n);
+    if (rc != PG_OK)
+        return rc;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
     *num_edges = edges;
     return PG_OK;
+}
+
+} // namespace pg
+
+extern "C" {
+
+int pg_version(void) { return 100; }
+
+const char *pg_last_error(void) { return pg::g_last_error.c_str(); }
+
+int pg_workspace_size(int64_t num_points, size_t *bytes)
+{
+    if (!bytes)
+        return pg::fail(PG_ERR_INVALID, "bytes must not be NULL");
+    if (num_points < 0 || num_points >= pg::kMaxPoints)
+        return pg::fail(PG_ERR_INVALID, "num_points must be in [0, 2^26)");
+    *bytes = pg::workspace_layout(num_points, 1, nullptr, nullptr);
+    return PG_OK;
+}
+
+int pg_build(int64_t n, const float *points, const float *weights, const int32_t *guesses, const int32_t *guess_off,
+             const pg_options *options, void *workspace, size_t workspace_bytes, int32_t *offsets, int32_t *status,
+             int64_t *num_edges, void *stream)
+{
+    if (!num_edges)
+        return pg::fail(PG_ERR_INVALID, "num_edges must not be NULL");
+    return pg::build_impl(n, 1, nullptr, points, weights, guesses, guess_off, options, workspace, workspace_bytes,
+                          offsets, status, num_edges, stream);
+}
+
+int pg_batch_workspace_size(int64_t total_points, int32_t num_clouds, size_t *bytes)
+{
+    if (!bytes || num_clouds < 1 || total_points < 0 || total_points >= pg::kMaxPoints)
+        return pg::fail(PG_ERR_INVALID, "need bytes != NULL, num_clouds >= 1 and total_points in [0, 2^26)");
+    *bytes = pg::workspace_layout(total_points, num_clouds, nullptr, nullptr);
+    return PG_OK;
+}
+
+int pg_build_batch(int64_t total_points, int32_t num_clouds, const int32_t *cloud_offsets, const float *points,
+                   const float *weights, const pg_options *options, void *workspace, size_t workspace_bytes,
+                   int32_t *offsets, int32_t *status, int64_t *num_edges, void *stream)
+{
+    if (num_clouds < 1 || !cloud_offsets)
+        return pg::fail(PG_ERR_INVALID, "num_clouds must be >= 1 and cloud_offsets must not be NULL");
+    return pg::build_impl(total_points, num_clouds, cloud_offsets, points, weights, nullptr, nullptr, options,
+                          workspace, workspace_bytes, offsets, status, num_edges, stream);
+}
+
+int pg_batch_check(const void *workspace, int64_t total_points, int32_t num_clouds, void *stream)
+{
+    using namespace pg;
+    if (!workspace || num_clouds < 1)
+        return fail(PG_ERR_INVALID, "bad arguments");
+    Workspace ws;
+    workspace_layout(total_points, num_clouds, (char *)workspace, &ws);
+    int host[4] = {0, 0, 0, 0};
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaMemcpyAsync(host, ws.counters, 4 * sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    return check_counters(host, total_points);
 }
 
 int pg_emit_adjacency(int64_t n, const void *workspace, const int32_t *offsets, int32_t *adjacency, void *stream)
@@ -300,7 +385,7 @@ int pg_emit_adjacency(int64_t n, const void *workspace, const int32_t *offsets, 
     if (!workspace || !offsets || !adjacency)
         return fail(PG_ERR_INVALID, "workspace, offsets and adjacency must not be NULL");
     Workspace ws;
-    workspace_layout(n, (char *)workspace, &ws);
+    workspace_layout(n, 1, (char *)workspace, &ws); // the CSR segments do not depend on the cloud count
     long long before = g_launches;
     csr_fill(ws, n, offsets, adjacency, (cudaStream_t)stream);
     g_profile[0] += (double)(g_launches - before);
@@ -325,7 +410,7 @@ int pg_stats(const void *workspace, int64_t n, uint64_t *out, int32_t count, voi
     if (!workspace || !out || count < 0)
         return fail(PG_ERR_INVALID, "bad arguments");
     Workspace ws;
-    workspace_layout(n, (char *)workspace, &ws);
+    workspace_layout(n, 1, (char *)workspace, &ws);
     unsigned long long tmp[kNumStats];
     cudaStream_t st = (cudaStream_t)stream;
     cudaMemcpyAsync(tmp, ws.stats, sizeof(tmp), cudaMemcpyDeviceToHost, st);

@@ -66,9 +66,11 @@ struct CellArgs
     const int *oid;
     const int *rank;
     const float4 *rec;
-    const float *box;
+    const float *box;        // 8 floats per cloud: reference box lo xyz, hi xyz, max weight
+    const int *cloud_off;    // [clouds + 1]
+    const int *cloud_root;   // [clouds]
+    int num_clouds;
     int n;
-    int root;
     int window;
     const int *guesses;
     const int *guess_off;
@@ -100,6 +102,8 @@ template <int CAP> struct WarpState
     int np;
     float4 s;
     int si, soid;
+    const float *box; // the cell's cloud box
+    int root;         // the cell's cloud BVH root
     float rsafe;
     int flags;
 };
@@ -247,7 +251,7 @@ __device__ __forceinline__ void cell_init(CellMem<CAP, STACK> &m, WarpState<CAP>
     {
         int ax = lane >> 1, hi = lane & 1;
         float sc = ax == 0 ? ws.s.x : (ax == 1 ? ws.s.y : ws.s.z);
-        float b = A.box[hi * 3 + ax];
+        float b = ws.box[hi * 3 + ax];
         float h = hi ? __fsub_rn(b, sc) : __fsub_rn(sc, b);
         float sg = hi ? 1.0f : -1.0f;
         m.pl[lane] = make_float4(ax == 0 ? sg : 0.0f, ax == 1 ? sg : 0.0f, ax == 2 ? sg : 0.0f, h);
@@ -404,7 +408,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
                 unsigned t = m.vt[slot];
                 int used = 0;
                 r = side_exact(m.pid[t & 255u], m.pid[(t >> 8) & 255u], m.pid[(t >> 16) & 255u], q.id, A.pts, A.oid,
-                               A.box, ws.s, ws.soid, &used);
+                               ws.box, ws.s, ws.soid, &used);
                 atomicAdd(&m.cnt[kStatFp64], 1ull);
                 if (used)
                     atomicAdd(&m.cnt[kStatExpansion], 1ull);
@@ -822,6 +826,11 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
     ws.s = A.pts[i];
     ws.si = i;
     ws.soid = A.oid[i];
+    {
+        int c = cloud_of(A.cloud_off, A.num_clouds, i);
+        ws.box = A.box + 8 * c;
+        ws.root = A.cloud_root[c];
+    }
     cell_init(m, ws, A, lane);
     const int n = A.n;
     const bool guessing = GUESS;
@@ -882,22 +891,22 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
     // empty sphere and, for a leaf, only the vertices that pass are pre-tested.
     const float4 *rec = A.rec;
     int sp = 0;
-    if (ref_is_leaf(A.root))
+    if (ref_is_leaf(ws.root))
     {
         VMask<CAP / 32> allv;
 #pragma unroll
         for (int k = 0; k < CAP / 32; ++k)
             allv.w[k] = 0xFFFFFFFFu;
-        if (!leaf_batch<CAP, STACK, GUESS>(m, ws, A.root, i, A, lane, allv))
+        if (!leaf_batch<CAP, STACK, GUESS>(m, ws, ws.root, i, A, lane, allv))
             return;
     }
     else
     {
         if (lane == 0)
         {
-            m.stk[0] = 0;
+            m.stk[0] = ws.root << 1;
             m.skey[0] = 0.0f;
-            m.stk[1] = 1;
+            m.stk[1] = (ws.root << 1) | 1;
             m.skey[1] = 0.0f;
         }
         sp = 2;
@@ -1114,6 +1123,8 @@ struct TCell
 {
     float4 s;
     int si, soid;
+    const float *box;
+    int root;
     int nv, np;
     float lx, ly, lz, ux, uy, uz; // bounding box of the exact cell, relative to the seed
     int flags;
@@ -1189,7 +1200,7 @@ __device__ __forceinline__ void t_init(TSlab &S, int lane, TCell &c, const CellA
     {
         int ax = code >> 1, hi = code & 1;
         float sc = ax == 0 ? c.s.x : (ax == 1 ? c.s.y : c.s.z);
-        float b = A.box[hi * 3 + ax];
+        float b = c.box[hi * 3 + ax];
         float h = hi ? __fsub_rn(b, sc) : __fsub_rn(sc, b);
         float sg = hi ? 1.0f : -1.0f;
         S.pl[code][lane] = make_float4(ax == 0 ? sg : 0.0f, ax == 1 ? sg : 0.0f, ax == 2 ? sg : 0.0f, h);
@@ -1266,7 +1277,7 @@ __device__ __forceinline__ int t_clip(TSlab &S, int lane, TCell &c, const Cand &
             unsigned t = S.vt[j][lane];
             int used = 0;
             r = side_exact(S.pid[t & 255u][lane], S.pid[(t >> 8) & 255u][lane], S.pid[(t >> 16) & 255u][lane], q.id,
-                           A.pts, A.oid, A.box, c.s, c.soid, &used);
+                           A.pts, A.oid, c.box, c.s, c.soid, &used);
             ++n_fp64;
             n_exp += used;
             if (r < 0)
@@ -1423,7 +1434,7 @@ __device__ __forceinline__ void t_process(TSlab &S, int lane, TCell &c, const Ce
         t_bounds(S, lane, c);
     int stk[kTStack];
     int sp = 0;
-    stk[sp++] = A.root;
+    stk[sp++] = c.root;
     while (sp > 0)
     {
         int ref = stk[--sp];
@@ -1550,6 +1561,11 @@ __global__ void __launch_bounds__(256, 4) k_tcells(CellArgs A, TSlab *slabs)
             c.si = (int)(A.begin + t);
             c.s = A.pts[c.si];
             c.soid = A.oid[c.si];
+            {
+                int cc = cloud_of(A.cloud_off, A.num_clouds, c.si);
+                c.box = A.box + 8 * cc;
+                c.root = A.cloud_root[cc];
+            }
             t_process(S, lane, c, A, ts);
             if (c.flags & kFlagError)
                 atomicExch(&A.counters[2], 1);
@@ -1592,8 +1608,10 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.rank = ws.rank;
     A.rec = ws.records;
     A.box = ws.box;
+    A.cloud_off = ws.cloud_off;
+    A.cloud_root = ws.cloud_root;
+    A.num_clouds = cl.num_clouds;
     A.n = (int)cl.n;
-    A.root = cl.root;
     A.window = cl.window;
     A.guesses = cl.guesses;
     A.guess_off = cl.guess_off;

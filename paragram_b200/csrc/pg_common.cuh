@@ -68,6 +68,21 @@ __host__ __device__ __forceinline__ int leaf_count(int r) { return ((r >> 26) & 
 
 constexpr int64_t kMaxPoints = (int64_t)1 << 26;
 
+// cloud of a point (original order) or of a sorted slot: clouds are contiguous in both
+__host__ __device__ __forceinline__ int cloud_of(const int *off, int num_clouds, int i)
+{
+    int lo = 0, hi = num_clouds;
+    while (hi - lo > 1)
+    {
+        int mid = (lo + hi) >> 1;
+        if (off[mid] <= i)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
 // float <-> order-preserving int for atomic min / max
 __device__ __forceinline__ int float_to_ordered(float f)
 {
@@ -83,9 +98,11 @@ __device__ __forceinline__ float ordered_to_float(int i) { return __int_as_float
 struct Workspace
 {
     // small header
-    int *bounds;          // [8]: ordered-int min xyz, max xyz, max w, unused
-    float *box;           // [8]: reference box lo xyz, hi xyz; Morton origin/scale in [6..7]
-    float *morton;        // [4]: origin xyz, scale
+    int *bounds;          // [8 per cloud]: ordered-int min xyz, max xyz, max w, unused
+    float *box;           // [8 per cloud]: reference box lo xyz, hi xyz, max weight
+    float *morton;        // [4 per cloud]: Morton origin xyz, extent
+    int *cloud_off;       // [clouds + 1]: first point of each cloud (original order = sorted order by cloud)
+    int *cloud_root;      // [clouds]: BVH root reference of each cloud
     int *counters;        // [16]: work counter, deferred count, error flag, edge total (2 ints), ...
     unsigned long long *stats; // [kNumStats]
     // LBVH
@@ -122,6 +139,6 @@ int big_warps();   // number of warps of the large-capacity pass
 size_t big_slab_bytes();
 int tcell_threads(); // resident threads of the thread-per-cell pass
 size_t tcell_slab_bytes();
-size_t workspace_layout(int64_t n, char *base, Workspace *ws);
+size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws);
 
 } // namespace pg

@@ -15,15 +15,15 @@ void exclusive_scan(const uint32_t *in, uint32_t *out, int64_t n, uint32_t *tmp,
 
 // pg_lbvh.cu
 int sort_blocks(int64_t n);
-void lbvh_build(const Workspace &ws, int64_t n, const float *points, const float *weights, int leaf_size,
-                cudaStream_t st);
+void lbvh_build(const Workspace &ws, int64_t n, int num_clouds, const float *points, const float *weights,
+                int leaf_size, cudaStream_t st);
 
 // pg_cells.cu
 struct CellLaunch
 {
     int64_t n;
     int leaf_size;
-    int root;                 // root reference (internal index or leaf code)
+    int num_clouds;           // independent point sets sharing the launch
     int window;               // warm-start half width (0: off)
     const int *guesses;       // initial guesses (original ids) or nullptr
     const int *guess_off;     // [N+1] offsets of the initial guesses

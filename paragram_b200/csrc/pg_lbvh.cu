@@ -28,59 +28,75 @@ constexpr int kSortTile = kSortThreads * kSortSteps;
 
 int sort_blocks(int64_t n) { return (int)((n + kSortTile - 1) / kSortTile); }
 
-__global__ void k_bounds_init(int *b)
+__global__ void k_bounds_init(int *b, int num_clouds)
 {
-    if (threadIdx.x < 3)
-        b[threadIdx.x] = float_to_ordered(INFINITY);
-    else if (threadIdx.x < 7)
-        b[threadIdx.x] = float_to_ordered(-INFINITY);
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= num_clouds * 8)
+        return;
+    int k = t & 7;
+    b[t] = float_to_ordered(k < 3 ? INFINITY : -INFINITY);
 }
 
-__global__ void k_bounds(const float *__restrict__ p, const float *__restrict__ w, int64_t n, int *b)
+// Per-cloud bounds: warps reduce per distinct cloud (normally one) before the atomics.
+__global__ void k_bounds(const float *__restrict__ p, const float *__restrict__ w, int64_t n,
+                         const int *__restrict__ coff, int num_clouds, int *b)
 {
-    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY}, mw = -INFINITY;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    const unsigned full = 0xFFFFFFFFu;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x)
     {
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
+        int64_t i = base + threadIdx.x;
+        bool ok = i < n;
+        int c = ok ? cloud_of(coff, num_clouds, (int)i) : -1;
+        float v[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (ok)
         {
-            float v = p[i * 3 + k];
-            mn[k] = fminf(mn[k], v);
-            mx[k] = fmaxf(mx[k], v);
+            v[0] = v[3] = p[i * 3 + 0];
+            v[1] = v[4] = p[i * 3 + 1];
+            v[2] = v[5] = p[i * 3 + 2];
+            v[6] = w ? w[i] : 0.0f;
         }
-        mw = fmaxf(mw, w ? w[i] : 0.0f);
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k)
-    {
-        int a = __reduce_min_sync(0xFFFFFFFFu, float_to_ordered(mn[k]));
-        int c = __reduce_max_sync(0xFFFFFFFFu, float_to_ordered(mx[k]));
-        if ((threadIdx.x & 31) == 0)
+        unsigned todo = __ballot_sync(full, ok);
+        while (todo)
         {
-            atomicMin(&b[k], a);
-            atomicMax(&b[3 + k], c);
+            int leader = __ffs(todo) - 1;
+            int cl = __shfl_sync(full, c, leader);
+            bool mine = ok && c == cl;
+            todo &= ~__ballot_sync(full, mine);
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+            {
+                int key = float_to_ordered(mine ? v[k] : (k < 3 ? INFINITY : -INFINITY));
+                int r = k < 3 ? __reduce_min_sync(full, key) : __reduce_max_sync(full, key);
+                if ((int)(threadIdx.x & 31) == leader)
+                {
+                    if (k < 3)
+                        atomicMin(&b[cl * 8 + k], r);
+                    else
+                        atomicMax(&b[cl * 8 + k], r);
+                }
+            }
         }
     }
-    int c = __reduce_max_sync(0xFFFFFFFFu, float_to_ordered(mw));
-    if ((threadIdx.x & 31) == 0)
-        atomicMax(&b[6], c);
 }
 
-// Reference box in FP32 (same operations as the reference) + Morton frame.
-__global__ void k_box(const int *b, float *box, float *morton)
+// Per cloud: the reference box in FP32 (same operations as the reference) and the Morton frame.
+__global__ void k_box(const int *b, float *box, float *morton, int num_clouds)
 {
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= num_clouds)
+        return;
     float mn[3], mx[3], ext = 0.0f;
     for (int k = 0; k < 3; ++k)
     {
-        mn[k] = ordered_to_float(b[k]);
-        mx[k] = ordered_to_float(b[3 + k]);
-        box[k] = __fsub_rn(__fsub_rn(mn[k], 1.0f), 1e-5f);
-        box[3 + k] = __fadd_rn(__fadd_rn(mx[k], 1.0f), 1e-5f);
+        mn[k] = ordered_to_float(b[c * 8 + k]);
+        mx[k] = ordered_to_float(b[c * 8 + 3 + k]);
+        box[c * 8 + k] = __fsub_rn(__fsub_rn(mn[k], 1.0f), 1e-5f);
+        box[c * 8 + 3 + k] = __fadd_rn(__fadd_rn(mx[k], 1.0f), 1e-5f);
         ext = fmaxf(ext, mx[k] - mn[k]);
-        morton[k] = mn[k];
+        morton[c * 4 + k] = mn[k];
     }
-    box[6] = ordered_to_float(b[6]); // max weight
-    morton[3] = ext > 0.0f ? 2097151.0f / ext : 0.0f;
+    box[c * 8 + 6] = ordered_to_float(b[c * 8 + 6]); // max weight
+    morton[c * 4 + 3] = ext;                          // extent; the scale depends on the bits per axis
 }
 
 __device__ __forceinline__ unsigned long long spread3(unsigned long long x)
@@ -94,23 +110,64 @@ __device__ __forceinline__ unsigned long long spread3(unsigned long long x)
     return x;
 }
 
-__device__ __forceinline__ unsigned long long quant(float v, float o, float s)
+__device__ __forceinline__ unsigned long long quant(float v, float o, float s, float top)
 {
     float t = (v - o) * s;
-    t = fminf(fmaxf(t, 0.0f), 2097151.0f);
+    t = fminf(fmaxf(t, 0.0f), top);
     return (unsigned long long)t;
 }
 
-__global__ void k_morton(const float *__restrict__ p, int64_t n, const float *__restrict__ morton,
-                         unsigned long long *__restrict__ keys, uint32_t *__restrict__ vals)
+// key = cloud id in the top bits, then a Morton code with `bits` bits per axis in the cloud's frame
+__global__ void k_morton(const float *__restrict__ p, int64_t n, const int *__restrict__ coff, int num_clouds,
+                         int bits, const float *__restrict__ morton, unsigned long long *__restrict__ keys,
+                         uint32_t *__restrict__ vals)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n)
         return;
-    float o0 = morton[0], o1 = morton[1], o2 = morton[2], s = morton[3];
-    unsigned long long x = quant(p[i * 3 + 0], o0, s), y = quant(p[i * 3 + 1], o1, s), z = quant(p[i * 3 + 2], o2, s);
-    keys[i] = (spread3(x) << 2) | (spread3(y) << 1) | spread3(z);
+    int c = cloud_of(coff, num_clouds, (int)i);
+    float top = (float)((1u << bits) - 1u);
+    float ext = morton[c * 4 + 3];
+    float sc = ext > 0.0f ? top / ext : 0.0f;
+    unsigned long long x = quant(p[i * 3 + 0], morton[c * 4 + 0], sc, top);
+    unsigned long long y = quant(p[i * 3 + 1], morton[c * 4 + 1], sc, top);
+    unsigned long long z = quant(p[i * 3 + 2], morton[c * 4 + 2], sc, top);
+    keys[i] = ((unsigned long long)c << (3 * bits)) | (spread3(x) << 2) | (spread3(y) << 1) | spread3(z);
     vals[i] = (uint32_t)i;
+}
+
+// Root of every cloud's subtree: clouds are contiguous in curve order (their id is
+// the key prefix), so each cloud with more than `leaf` points is one Karras subtree.
+__global__ void k_cloud_roots(const int *__restrict__ coff, int num_clouds, int leaf, const int *__restrict__ first,
+                              const int *__restrict__ last, const int *__restrict__ parent_int,
+                              const int *__restrict__ parent_leaf, int *__restrict__ roots, int *err)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= num_clouds)
+        return;
+    int a = coff[c], b = coff[c + 1], nc = b - a;
+    if (nc <= 0)
+    {
+        roots[c] = 0;
+        return;
+    }
+    if (nc <= leaf)
+    {
+        roots[c] = leaf_ref(a, nc);
+        return;
+    }
+    int node = parent_leaf[a];
+    for (int it = 0; it < 200 && node >= 0; ++it)
+    {
+        if (first[node] == a && last[node] == b - 1)
+        {
+            roots[c] = node;
+            return;
+        }
+        node = parent_int[node];
+    }
+    roots[c] = 0;
+    atomicExch(err, 2);
 }
 
 // ---------------------------------------------------------------------------
@@ -345,21 +402,25 @@ __global__ void k_records(const float4 *__restrict__ pts, int64_t n, const int *
     rec[4 * (size_t)i + 3] = make_float4(__int_as_float(cref[0]), __int_as_float(cref[1]), clo[0].w, clo[1].w);
 }
 
-void lbvh_build(const Workspace &ws, int64_t n, const float *points, const float *weights, int leaf_size,
-                cudaStream_t st)
+void lbvh_build(const Workspace &ws, int64_t n, int num_clouds, const float *points, const float *weights,
+                int leaf_size, cudaStream_t st)
 {
     ++g_launches;
-    k_bounds_init<<<1, 32, 0, st>>>(ws.bounds);
+    k_bounds_init<<<(num_clouds * 8 + 255) / 256, 256, 0, st>>>(ws.bounds, num_clouds);
     int nb = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
     if (nb < 1)
         nb = 1;
     ++g_launches;
-    k_bounds<<<nb, 256, 0, st>>>(points, weights, n, ws.bounds);
+    k_bounds<<<nb, 256, 0, st>>>(points, weights, n, ws.cloud_off, num_clouds, ws.bounds);
     ++g_launches;
-    k_box<<<1, 1, 0, st>>>(ws.bounds, ws.box, ws.morton);
+    k_box<<<(num_clouds + 127) / 128, 128, 0, st>>>(ws.bounds, ws.box, ws.morton, num_clouds);
+    int cbits = 0;
+    while ((1 << cbits) < num_clouds)
+        ++cbits;
+    int bits = std::min(21, (63 - cbits) / 3);
     unsigned g = (unsigned)((n + 255) / 256);
     ++g_launches;
-    k_morton<<<g, 256, 0, st>>>(points, n, ws.morton, ws.keys0, ws.vals0);
+    k_morton<<<g, 256, 0, st>>>(points, n, ws.cloud_off, num_clouds, bits, ws.morton, ws.keys0, ws.vals0);
     int blocks = sort_blocks(n);
     unsigned long long *ka = ws.keys0, *kb = ws.keys1;
     uint32_t *va = ws.vals0, *vb = ws.vals1;
@@ -387,6 +448,10 @@ void lbvh_build(const Workspace &ws, int64_t n, const float *points, const float
         ++g_launches;
         k_records<<<g, 256, 0, st>>>(ws.pts, n, ws.left, ws.right, ws.first, ws.nbox, leaf_size, ws.records);
     }
+    ++g_launches;
+    k_cloud_roots<<<(num_clouds + 127) / 128, 128, 0, st>>>(ws.cloud_off, num_clouds, leaf_size, ws.first, ws.last,
+                                                            ws.parent_int, ws.parent_leaf, ws.cloud_root,
+                                                            &ws.counters[2]);
 }
 
 } // namespace pg

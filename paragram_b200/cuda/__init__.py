@@ -36,7 +36,7 @@ def _check(ok: bool, msg: str):
 
 def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug: bool,
          initial_guesses: Optional[torch.Tensor], initial_guesses_offsets: Optional[torch.Tensor], leaf_size: int,
-         num_chunks: int = 0, stats: bool = False, profile: bool = False):
+         num_chunks: int = 0, stats: bool = False, profile: bool = False, blocks_per_sm: int = 0):
     n = int(points.shape[0])
     _check(points.device.type == "cuda", "points must be on CUDA device")
     _check(points.dtype == torch.float32, "points must be of type float")
@@ -61,7 +61,8 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
         if initial_guesses.numel() == 0:
             initial_guesses = torch.zeros(1, dtype=torch.int32, device=dev)
         gptr, optr = initial_guesses.data_ptr(), initial_guesses_offsets.data_ptr()
-    opts = _lib.PgOptions(int(knn), int(leaf_size), int(bool(debug)) | (2 if profile else 0), int(num_chunks))
+    opts = _lib.PgOptions(int(knn), int(leaf_size), int(bool(debug)) | (2 if profile else 0), int(num_chunks),
+                          int(blocks_per_sm))
     with torch.cuda.device(dev):
         nbytes = ctypes.c_size_t(0)
         rc = _LIB.pg_workspace_size(n, ctypes.byref(nbytes))
@@ -111,14 +112,14 @@ def build_laguerre_voronoi_ultra(points: torch.Tensor, weights: torch.Tensor, kn
 
 
 def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = None, *, knn: int = 8,
-                     leaf_size: int = -1, num_chunks: int = 0, profile: bool = False,
+                     leaf_size: int = -1, num_chunks: int = 0, profile: bool = False, blocks_per_sm: int = 0,
                      initial_guesses: Optional[torch.Tensor] = None,
                      initial_guesses_offsets: Optional[torch.Tensor] = None):
     """Build and return ``((adjacency, offsets, status), counters)``; counters as in ``STAT_NAMES``."""
     if weights is not None and weights.dim() == 1:
         weights = weights[:, None]
     res = _run(points, weights, knn, False, initial_guesses, initial_guesses_offsets, leaf_size,
-               num_chunks=num_chunks, stats=True, profile=profile)
+               num_chunks=num_chunks, stats=True, profile=profile, blocks_per_sm=blocks_per_sm)
     return res, dict(_last_stats)
 
 
