@@ -62,6 +62,14 @@ typedef struct pg_options
     int32_t blocks_per_sm; /* register budget of the cell kernel: resident blocks of 8 warps per SM
                               (2 or 3; 0 = default 2). No reference counterpart; chosen by the
                               autotuner. Results do not depend on it. */
+    int32_t reserved;      /* must be 0 */
+    const void *model;     /* learned search radius: device pointer to a pg_model, or NULL for the
+                              plain traversal. No reference counterpart. Results do not depend on it. */
+    float *radius_out;     /* device float32 [num_points] or NULL: per point, the certified radius of its
+                              final cell (max distance of a vertex from the point, power-adjusted;
+                              0 for an empty cell). Training targets of the learned radius. */
+    int32_t *work_out;     /* device int32 [4 * num_points] or NULL: per point, BVH nodes visited, leaves
+                              visited, candidates tested and the peak length of the node queue. */
 } pg_options;
 
 /* Library version (major * 10000 + minor * 100 + patch). */
@@ -82,7 +90,8 @@ int pg_workspace_size(int64_t num_points, size_t *bytes);
  *   initial_guesses / initial_guesses_offsets
  *               int32 CSR of candidate neighbours per point (original ids), or both NULL
  *               (reference: voronoi_ultra.cu:69-85). Results do not depend on them.
- *   options     host pointer or NULL (defaults: knn 8, leaf_size -1, debug 0, num_chunks 0, blocks_per_sm 0)
+ *   options     host pointer or NULL (defaults: knn 8, leaf_size -1, debug 0, num_chunks 0, blocks_per_sm 0,
+ *               no model, no per-point diagnostics)
  *   workspace   device buffer of at least pg_workspace_size() bytes, 256-byte aligned;
  *               it must stay alive until pg_emit_adjacency returns
  *   offsets     int32 [num_points + 1]  (output)

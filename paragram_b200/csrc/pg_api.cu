@@ -166,7 +166,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
 {
     g_last_error.clear();
     cudaStream_t st = (cudaStream_t)stream;
-    pg_options opt = {8, -1, 0, 0, 0};
+    pg_options opt = {8, -1, 0, 0, 0, 0, nullptr, nullptr, nullptr};
     if (options)
         opt = *options;
     const bool sync = num_edges != nullptr;
@@ -182,6 +182,10 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         return fail(PG_ERR_INVALID, "workspace must be 256-byte aligned");
     if (opt.leaf_size > kMaxLeaf)
         return fail(PG_ERR_INVALID, "leaf_size must be at most 32");
+    if (opt.reserved != 0)
+        return fail(PG_ERR_INVALID, "options.reserved must be 0");
+    if (((uintptr_t)opt.work_out & 15u) != 0 || ((uintptr_t)opt.radius_out & 3u) != 0)
+        return fail(PG_ERR_INVALID, "work_out must be 16-byte and radius_out 4-byte aligned");
     size_t need = workspace_layout(n, num_clouds, nullptr, nullptr);
     if (workspace_bytes < need)
         return fail(PG_ERR_INVALID, "workspace too small: need " + std::to_string(need) + " bytes");
@@ -242,6 +246,8 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         cl.min_blocks = mb ? std::atoi(mb) : (opt.blocks_per_sm == 3 ? 3 : 2);
         cl.big_cap = big_cap(n);
     }
+    cl.radius_out = opt.radius_out;
+    cl.work_out = opt.work_out;
     int chunks = sync ? plan_chunks(n, opt.num_chunks) : std::max(opt.num_chunks, 1);
     int sms = device_sms();
     int64_t per = (n + chunks - 1) / chunks;
@@ -316,7 +322,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
 
 extern "C" {
 
-int pg_version(void) { return 100; }
+int pg_version(void) { return 101; }
 
 const char *pg_last_error(void) { return pg::g_last_error.c_str(); }
 

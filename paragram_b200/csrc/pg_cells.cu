@@ -44,6 +44,11 @@ namespace pg
 {
 
 constexpr float kEps = 5.9604645e-8f; // 2^-24
+// A vertex whose FP32 error radius exceeds this fraction of its L1 norm is rebuilt in FP64.
+#ifndef PG_VERTEX64_REL
+#define PG_VERTEX64_REL 3e-4f
+#endif
+constexpr float kVertex64Rel = PG_VERTEX64_REL;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 template <int CAP, int STACK> struct CellMem
@@ -58,6 +63,7 @@ template <int CAP, int STACK> struct CellMem
     int stk[STACK];   // pending BVH references (unordered)
     float skey[STACK]; // lower bound of the bisector distance of any point of the pending node
     unsigned long long cnt[kNumStats]; // per-warp statistics (written by lane 0)
+    unsigned long long cnt0[3];        // nodes, leaves, candidates at the start of the current cell
 };
 
 struct CellArgs
@@ -86,6 +92,8 @@ struct CellArgs
     int64_t big_cap;
     char *slabs;
     int inline_big; // rebuild deferred cells right away in the same kernel (warp path)
+    float *radius_out; // optional per-cell diagnostics (original ids)
+    int4 *work_out;
 };
 
 enum Flag : int
@@ -106,6 +114,7 @@ template <int CAP> struct WarpState
     int root;         // the cell's cloud BVH root
     float rsafe;
     int flags;
+    int peak; // longest node queue of the current cell
 };
 
 // statistics live in the warp's shared-memory block, not in registers
@@ -118,6 +127,14 @@ template <int CAP> struct WarpState
             (m).cnt[idx] += pg_count_v_;                                                                               \
     } while (0)
 
+// Optional per-phase SM cycle counters (compile with -DPG_PHASE_CYCLES).
+#ifdef PG_PHASE_CYCLES
+#define PG_T0(t) long long t = clock64()
+#define PG_T1(m, lane, idx, t) PG_COUNT(m, lane, idx, clock64() - (t))
+#else
+#define PG_T0(t)
+#define PG_T1(m, lane, idx, t)
+#endif
 
 struct Cand
 {
@@ -168,23 +185,26 @@ __device__ __forceinline__ int side_fp32(float4 X, const Cand &q)
     return g > b ? 1 : (g < -b ? 0 : -1);
 }
 
-__device__ __forceinline__ exact::PlaneSrc plane_src(int pid, const CellArgs &A)
+// Source of plane `pid` (a sorted point index, or -1 - box code) of a cell
+// whose cloud box is `box`.
+__device__ __forceinline__ exact::PlaneSrc plane_src(int pid, const float4 *__restrict__ pts,
+                                                     const int *__restrict__ oid, const float *__restrict__ box)
 {
     exact::PlaneSrc r;
     if (pid >= 0)
     {
-        float4 p = A.pts[pid];
+        float4 p = pts[pid];
         r.x = p.x;
         r.y = p.y;
         r.z = p.z;
         r.w = p.w;
         r.box = -1;
-        r.oid = A.oid[pid];
+        r.oid = oid[pid];
     }
     else
     {
         int code = -1 - pid;
-        r.x = A.box[(code & 1) * 3 + (code >> 1)];
+        r.x = box[(code & 1) * 3 + (code >> 1)];
         r.y = r.z = r.w = 0.0f;
         r.box = code;
         r.oid = -1;
@@ -198,12 +218,8 @@ __device__ __noinline__ int side_exact(int p0, int p1, int p2, int qid, const fl
                                        const int *__restrict__ oid, const float *__restrict__ box, float4 s, int soid,
                                        int *used)
 {
-    CellArgs A;
-    A.pts = pts;
-    A.oid = oid;
-    A.box = box;
-    exact::PlaneSrc vp[3] = {plane_src(p0, A), plane_src(p1, A), plane_src(p2, A)};
-    exact::PlaneSrc cp = plane_src(qid, A);
+    exact::PlaneSrc vp[3] = {plane_src(p0, pts, oid, box), plane_src(p1, pts, oid, box), plane_src(p2, pts, oid, box)};
+    exact::PlaneSrc cp = plane_src(qid, pts, oid, box);
     return exact::side_test(vp, cp, s.x, s.y, s.z, s.w, soid, used);
 }
 
@@ -228,19 +244,88 @@ __device__ __forceinline__ float4 make_vertex(float4 a, float ea, float4 b, floa
     float ra = fabsf(__fmaf_rn(a.x, X, __fmaf_rn(a.y, Y, __fmaf_rn(a.z, Z, -a.w)))) + 4.0f * kEps * (la * xn + fabsf(a.w)) + ea;
     float rb = fabsf(__fmaf_rn(b.x, X, __fmaf_rn(b.y, Y, __fmaf_rn(b.z, Z, -b.w)))) + 4.0f * kEps * (lb * xn + fabsf(b.w)) + eb;
     float rc = fabsf(__fmaf_rn(c.x, X, __fmaf_rn(c.y, Y, __fmaf_rn(c.z, Z, -c.w)))) + 4.0f * kEps * (lc * xn + fabsf(c.w)) + ec;
-    float r2 = ra * ra + rb * rb + rc * rc;
-    float rho = r2 > 0.0f ? r2 * rsqrtf(r2) * (1.0f + 4e-6f) : 0.0f;
-    float f2 = u0x * u0x + u0y * u0y + u0z * u0z + u1x * u1x + u1y * u1y + u1z * u1z + u2x * u2x + u2y * u2y +
-               u2z * u2z;
-    float F = (f2 > 0.0f ? f2 * rsqrtf(f2) * (1.0f + 4e-6f) : 0.0f) + 8.0f * kEps * (lb * lc + lc * la + la * lb);
+    // X - X_exact = adj(A) r / D with the columns u0, u1, u2 of adj(A) and the residuals r, so
+    // |X - X_exact| <= (ra |u0| + rb |u1| + rc |u2|) / |D|, each |u_i| bounded with its rounding
+    // error (2 eps per product pair). Per-plane weighting keeps the bound tight for a vertex far
+    // along a thin prism, whose large-offset box plane only moves it along the prism axis.
+    float q0 = u0x * u0x + u0y * u0y + u0z * u0z;
+    float q1 = u1x * u1x + u1y * u1y + u1z * u1z;
+    float q2 = u2x * u2x + u2y * u2y + u2z * u2z;
+    float U0 = (q0 > 0.0f ? q0 * rsqrtf(q0) * (1.0f + 4e-6f) : 0.0f) + 8.0f * kEps * lb * lc;
+    float U1 = (q1 > 0.0f ? q1 * rsqrtf(q1) * (1.0f + 4e-6f) : 0.0f) + 8.0f * kEps * lc * la;
+    float U2 = (q2 > 0.0f ? q2 * rsqrtf(q2) * (1.0f + 4e-6f) : 0.0f) + 8.0f * kEps * la * lb;
+    float num = (ra * U0 + rb * U1 + rc * U2) * (1.0f + 4e-6f);
     float den = fabsf(D) - 8.0f * kEps * la * lb * lc;
-    float ex = den > 0.0f ? __fdividef(F * rho, den) * (1.0f + 4e-6f) : INFINITY;
+    float ex = den > 0.0f ? __fdividef(num, den) * (1.0f + 4e-6f) : INFINITY;
     float psi = (2.0f * ex + 4.0f * kEps * xn) * (1.0f + 1e-6f);
     if (!(psi < 1e30f) || !(xn < 1e30f))
         psi = INFINITY;
     float r = xn + psi;
     vr = r * r * (1.0f + 1e-6f);
     return make_float4(X, Y, Z, psi);
+}
+
+// Vertex of three planes rebuilt in FP64 from the planes' sources (the FP32
+// plane coefficients are themselves rounded), for a vertex whose FP32 error
+// radius is large: three nearly dependent planes, e.g. two bisectors of
+// near-coplanar points meeting a third along a long thin cell. Returns the FP32
+// point with psi = 2 * (FP64 a-posteriori bound) + |X32 - X64| + the FP32
+// side-test rounding term, or `fallback` when a plane is not exact in FP64.
+__device__ __noinline__ float4 make_vertex64(int pid0, int pid1, int pid2, const float4 *__restrict__ pts,
+                                             const int *__restrict__ oid, const float *__restrict__ box, float4 s,
+                                             float4 fallback, float fallback_vr, float &vr)
+{
+    const double u = 1.1102230246251565e-16; // 2^-53
+    exact::DRow r[3];
+    exact::make_drow(plane_src(pid0, pts, oid, box), s.x, s.y, s.z, s.w, r[0]);
+    exact::make_drow(plane_src(pid1, pts, oid, box), s.x, s.y, s.z, s.w, r[1]);
+    exact::make_drow(plane_src(pid2, pts, oid, box), s.x, s.y, s.z, s.w, r[2]);
+    if (!(r[0].ok && r[1].ok && r[2].ok))
+    {
+        vr = fallback_vr;
+        return fallback;
+    }
+    // plane i: a_i . X = b_i / 2 with |b_i - b_i exact| <= eb_i
+    const double *a = r[0].a, *b = r[1].a, *c = r[2].a;
+    double u0x = b[1] * c[2] - b[2] * c[1], u0y = b[2] * c[0] - b[0] * c[2], u0z = b[0] * c[1] - b[1] * c[0];
+    double u1x = c[1] * a[2] - c[2] * a[1], u1y = c[2] * a[0] - c[0] * a[2], u1z = c[0] * a[1] - c[1] * a[0];
+    double u2x = a[1] * b[2] - a[2] * b[1], u2y = a[2] * b[0] - a[0] * b[2], u2z = a[0] * b[1] - a[1] * b[0];
+    double D = a[0] * u0x + a[1] * u0y + a[2] * u0z;
+    double h0 = 0.5 * r[0].b, h1 = 0.5 * r[1].b, h2 = 0.5 * r[2].b;
+    double X = (h0 * u0x + h1 * u1x + h2 * u2x) / D;
+    double Y = (h0 * u0y + h1 * u1y + h2 * u2y) / D;
+    double Z = (h0 * u0z + h1 * u1z + h2 * u2z) / D;
+    double la = fabs(a[0]) + fabs(a[1]) + fabs(a[2]);
+    double lb = fabs(b[0]) + fabs(b[1]) + fabs(b[2]);
+    double lc = fabs(c[0]) + fabs(c[1]) + fabs(c[2]);
+    double xn = sqrt(X * X + Y * Y + Z * Z) * (1.0 + 1e-14);
+    double ra = fabs(fma(a[0], X, fma(a[1], Y, fma(a[2], Z, -h0)))) + 4.0 * u * (la * xn + fabs(h0)) + 0.5 * r[0].eb;
+    double rb = fabs(fma(b[0], X, fma(b[1], Y, fma(b[2], Z, -h1)))) + 4.0 * u * (lb * xn + fabs(h1)) + 0.5 * r[1].eb;
+    double rc = fabs(fma(c[0], X, fma(c[1], Y, fma(c[2], Z, -h2)))) + 4.0 * u * (lc * xn + fabs(h2)) + 0.5 * r[2].eb;
+    double U0 = sqrt(u0x * u0x + u0y * u0y + u0z * u0z) * (1.0 + 1e-14) + 4.0 * u * lb * lc;
+    double U1 = sqrt(u1x * u1x + u1y * u1y + u1z * u1z) * (1.0 + 1e-14) + 4.0 * u * lc * la;
+    double U2 = sqrt(u2x * u2x + u2y * u2y + u2z * u2z) * (1.0 + 1e-14) + 4.0 * u * la * lb;
+    double den = fabs(D) - 8.0 * u * la * lb * lc;
+    if (!(den > 0.0) || !(xn < 1e30))
+    {
+        vr = fallback_vr;
+        return fallback;
+    }
+    double ex = (ra * U0 + rb * U1 + rc * U2) / den * (1.0 + 1e-13);
+    float fx = (float)X, fy = (float)Y, fz = (float)Z;
+    double dx = (double)fx - X, dy = (double)fy - Y, dz = (double)fz - Z;
+    double e32 = sqrt(dx * dx + dy * dy + dz * dz) * (1.0 + 1e-14);
+    float x2 = fx * fx + fy * fy + fz * fz;
+    float xnf = x2 > 0.0f ? x2 * rsqrtf(x2) * (1.0f + 4e-6f) : 0.0f;
+    float psi = (float)((2.0 * ex + e32) * (1.0 + 1e-6)) * (1.0f + 1e-6f) + 4.0f * kEps * xnf;
+    if (!(psi < fallback.w))
+    {
+        vr = fallback_vr;
+        return fallback;
+    }
+    float rr = xnf + psi;
+    vr = rr * rr * (1.0f + 1e-6f);
+    return make_float4(fx, fy, fz, psi);
 }
 
 template <int CAP, int STACK>
@@ -556,6 +641,27 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
                 ws.flags |= kFlagError; // unreachable: capacity was checked above
         }
     }
+    // ill-conditioned in FP32: rebuild in FP64 so that the empty sphere stays tight
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+    {
+        unsigned mm = nbits[k];
+        while (mm)
+        {
+            int slot = k * 32 + __ffs(mm) - 1;
+            mm &= mm - 1;
+            float4 X = m.vx[slot];
+            if (!(X.w <= kVertex64Rel * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z))))
+            {
+                unsigned t = m.vt[slot];
+                float vr = m.vr[slot];
+                m.vx[slot] = make_vertex64(m.pid[t & 255u], m.pid[(t >> 8) & 255u], m.pid[(t >> 16) & 255u], A.pts, A.oid,
+                                           ws.box, ws.s, X, vr, vr);
+                m.vr[slot] = vr;
+                atomicAdd(&m.cnt[kStatVertex64], 1ull);
+            }
+        }
+    }
 #pragma unroll
     for (int k = 0; k < W; ++k)
         ws.valid[k] = (ws.valid[k] & ~rem[k]) | __reduce_or_sync(kFull, nbits[k]);
@@ -616,7 +722,9 @@ __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP>
         int src = (int)(mn & 31u);
         todo &= ~(1u << src);
         Cand c = shfl_cand(q, src);
+        PG_T0(tc);
         int r = clip(m, ws, c, A, lane);
+        PG_T1(m, lane, kStatCycClips, tc);
         if (r == kClipEmptied)
             return false;
         if (r == kClipDefer)
@@ -832,8 +940,16 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
         ws.root = A.cloud_root[c];
     }
     cell_init(m, ws, A, lane);
+    ws.peak = 0;
+    if (A.work_out != nullptr && lane == 0)
+    {
+        m.cnt0[0] = m.cnt[kStatNodes];
+        m.cnt0[1] = m.cnt[kStatLeaves];
+        m.cnt0[2] = m.cnt[kStatCandidates];
+    }
     const int n = A.n;
     const bool guessing = GUESS;
+    PG_T0(tw);
     // 1. warm start: curve-order neighbours (or the caller's initial guesses)
     if (guessing)
     {
@@ -884,6 +1000,7 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
         if (!run_batch(m, ws, have, q, key, A, lane, VMask<CAP / 32>{}, false))
             return;
     }
+    PG_T1(m, lane, kStatCycWarm, tw);
     // 2. BVH traversal, best first. A pending entry is (parent << 1 | side) with
     // a lower bound of the bisector distance of the child's points; the entry
     // with the smallest bound is popped, dropped if the bound exceeds the radius
@@ -914,11 +1031,18 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
     __syncwarp();
     while (sp > 0)
     {
-        unsigned best = 0xFFFFFFFFu;
-        for (int j = lane; j < sp; j += 32)
-            best = min(best, (__float_as_uint(m.skey[j]) & ~(unsigned)(STACK - 1)) | (unsigned)j);
-        best = __reduce_min_sync(kFull, best);
-        int jb = (int)(best & (unsigned)(STACK - 1));
+        PG_T0(tn);
+        int jb = sp - 1;
+        if (sp <= STACK - 64)
+        {
+            unsigned best = 0xFFFFFFFFu;
+            for (int j = lane; j < sp; j += 32)
+                best = min(best, (__float_as_uint(m.skey[j]) & ~(unsigned)(STACK - 1)) | (unsigned)j);
+            best = __reduce_min_sync(kFull, best);
+            jb = (int)(best & (unsigned)(STACK - 1));
+        }
+        // else: a nearly full queue continues depth first (newest entry), which adds at most one
+        // pending entry per tree level; the order of visits never changes the cell.
         int ent = m.stk[jb];
         float key = m.skey[jb];
         __syncwarp();
@@ -930,7 +1054,10 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
         --sp;
         __syncwarp();
         if (key > ws.rsafe)
+        {
+            PG_T1(m, lane, kStatCycNodes, tn);
             continue;
+        }
         PG_COUNT(m, lane, kStatNodes, 1);
         int parent = ent >> 1, side = ent & 1;
         const float4 *r = rec + 4 * (size_t)parent;
@@ -949,15 +1076,19 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
         }
         VMask<CAP / 32> vm;
         bool any = node_vertex_mask(m, ws, lx, ly, lz, hx, hy, hz, mw, lane, vm);
+        PG_T1(m, lane, kStatCycNodes, tn);
         if (!any)
             continue;
         if (ref_is_leaf(ref))
         {
+            PG_T0(tl);
             bool go = leaf_batch<CAP, STACK, GUESS>(m, ws, ref, i, A, lane, vm);
+            PG_T1(m, lane, kStatCycLeaves, tl);
             if (!go)
                 return;
             continue;
         }
+        PG_T0(tn2);
         // internal: queue both children with their distance bounds
         const float4 *rc = rec + 4 * (size_t)ref;
         float4 c0 = rc[0], c1 = rc[1], c2 = rc[2], c3 = rc[3];
@@ -984,8 +1115,24 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
             }
         }
         sp += (p0 ? 1 : 0) + (p1 ? 1 : 0);
+        ws.peak = max(ws.peak, sp);
         __syncwarp();
+        PG_T1(m, lane, kStatCycNodes, tn2);
     }
+}
+
+// Optional per-cell diagnostics: certified radius and traversal work.
+template <int CAP, int STACK>
+__device__ __forceinline__ void write_diagnostics(const CellMem<CAP, STACK> &m, const WarpState<CAP> &ws,
+                                                  const CellArgs &A, int lane)
+{
+    if (lane != 0)
+        return;
+    if (A.radius_out != nullptr)
+        A.radius_out[ws.soid] = (ws.flags & kFlagEmpty) ? 0.0f : ws.rsafe;
+    if (A.work_out != nullptr)
+        A.work_out[ws.soid] = make_int4((int)(m.cnt[kStatNodes] - m.cnt0[0]), (int)(m.cnt[kStatLeaves] - m.cnt0[1]),
+                                        (int)(m.cnt[kStatCandidates] - m.cnt0[2]), ws.peak);
 }
 
 template <int CAP, int STACK> __device__ void flush_stats(CellMem<CAP, STACK> &m, const CellArgs &A, int lane)
@@ -1012,6 +1159,7 @@ template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, i
     slot = __shfl_sync(kFull, slot, 0);
     __syncwarp();
     process_cell<kCapBig, kStackBig, GUESS>(m, ws, i, A, lane);
+    write_diagnostics(m, ws, A, lane);
     if ((ws.flags & kFlagError) && lane == 0)
         atomicExch(&A.counters[2], 1);
     if (slot < A.big_cap)
@@ -1046,7 +1194,9 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
         if (t >= count)
             break;
         int i = A.big_pass ? A.big_list[t] : (int)(A.begin + t);
+        PG_T0(tcell);
         process_cell<CAP, STACK, GUESS>(m, ws, i, A, lane);
+        write_diagnostics(m, ws, A, lane);
         if (A.big_pass)
             ws.si = t; // the deferred-row slot
         if (ws.flags & kFlagError)
@@ -1056,12 +1206,21 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
             ws.flags &= ~kFlagError;
         }
         if (!(ws.flags & kFlagDefer) || A.big_pass)
-            if (write_outputs(m, ws, A, lane, A.big_pass != 0))
+        {
+            PG_T0(to);
+            bool done = write_outputs(m, ws, A, lane, A.big_pass != 0);
+            PG_T1(m, lane, kStatCycOut, to);
+            if (done)
+            {
+                PG_T1(m, lane, kStatCycCell, tcell);
                 continue;
+            }
+        }
         PG_COUNT(m, lane, kStatDeferred, 1);
         if (A.inline_big)
         {
             big_cell<GUESS>(A, i, lane);
+            PG_T1(m, lane, kStatCycCell, tcell);
             continue;
         }
         // deferred: placeholder outputs (an empty row) until the large-capacity pass
@@ -1628,6 +1787,8 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.big_cap = 0;
     A.slabs = (char *)ws.big_slabs;
     A.inline_big = 0;
+    A.radius_out = cl.radius_out;
+    A.work_out = reinterpret_cast<int4 *>(cl.work_out);
     return A;
 }
 

@@ -53,7 +53,8 @@ enum Stat : int
     kStatCycOut = 13,    // row output
     kStatDeferVerts = 14,  // deferrals / large-pass overflows: vertex or plane slots
     kStatDeferStack = 15,  // deferrals / large-pass overflows: traversal stack
-    kNumStats = 16,
+    kStatVertex64 = 16,    // vertices rebuilt in FP64 (ill-conditioned in FP32)
+    kNumStats = 17,
 };
 
 // leaf reference encoding in BVH records: bit 31 set, count-1 in bits 26..30,

@@ -31,6 +31,8 @@ struct CellLaunch
     int weighted;
     int min_blocks; // register-budget variant of the cell kernel (2, 3 or 4 blocks per SM)
     int64_t big_cap; // deferred-row slots
+    float *radius_out; // per original id: certified radius of the final cell, or nullptr
+    int *work_out;     // per original id: nodes, leaves, candidates, peak queue; or nullptr
 };
 void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int num_sms, cudaStream_t st);
 void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st);

@@ -23,8 +23,9 @@ _LIB = _lib.load()
 #: Counter names returned by ``last_stats()`` (pg_stats in include/paragram_b200.h).
 STAT_NAMES = ["tests", "fp64_escalations", "exact_escalations", "deferred_cells", "nodes", "leaves", "clips",
               "candidates", "cyc_cell", "cyc_warm", "cyc_nodes", "cyc_leaves", "cyc_clips", "cyc_out", "defer_slots",
-              "defer_stack"]
+              "defer_stack", "vertex64"]
 _last_stats: dict = {}
+_last_diag: dict = {}
 #: Names of the values returned by ``last_profile()`` (pg_last_profile in include/paragram_b200.h).
 PROFILE_NAMES = ["launches", "lbvh_ms", "cells_ms", "deferred_ms", "csr_ms", "deferred_cells", "chunks"]
 
@@ -36,7 +37,8 @@ def _check(ok: bool, msg: str):
 
 def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug: bool,
          initial_guesses: Optional[torch.Tensor], initial_guesses_offsets: Optional[torch.Tensor], leaf_size: int,
-         num_chunks: int = 0, stats: bool = False, profile: bool = False, blocks_per_sm: int = 0):
+         num_chunks: int = 0, stats: bool = False, profile: bool = False, blocks_per_sm: int = 0,
+         diagnostics: bool = False, model: Optional[torch.Tensor] = None):
     n = int(points.shape[0])
     _check(points.device.type == "cuda", "points must be on CUDA device")
     _check(points.dtype == torch.float32, "points must be of type float")
@@ -63,6 +65,15 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
         gptr, optr = initial_guesses.data_ptr(), initial_guesses_offsets.data_ptr()
     opts = _lib.PgOptions(int(knn), int(leaf_size), int(bool(debug)) | (2 if profile else 0), int(num_chunks),
                           int(blocks_per_sm))
+    if model is not None:
+        _check(model.device == dev and model.dtype == torch.uint8 and model.is_contiguous(),
+               "model must be a contiguous uint8 tensor (a packed pg_model) on the points' device")
+        opts.model = model.data_ptr()
+    radius = work = None
+    if diagnostics:
+        radius = torch.zeros(max(n, 1), dtype=torch.float32, device=dev)
+        work = torch.zeros(max(n, 1), 4, dtype=torch.int32, device=dev)
+        opts.radius_out, opts.work_out = radius.data_ptr(), work.data_ptr()
     with torch.cuda.device(dev):
         nbytes = ctypes.c_size_t(0)
         rc = _LIB.pg_workspace_size(n, ctypes.byref(nbytes))
@@ -87,6 +98,9 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
             _check(rc == 0, _lib.last_error(_LIB))
             _last_stats.clear()
             _last_stats.update({k: int(v) for k, v in zip(STAT_NAMES, out)})
+    _last_diag.clear()
+    if diagnostics:
+        _last_diag.update(radius=radius[:n], work=work[:n])
     return adjacency, offsets, status
 
 
@@ -114,13 +128,22 @@ def build_laguerre_voronoi_ultra(points: torch.Tensor, weights: torch.Tensor, kn
 def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = None, *, knn: int = 8,
                      leaf_size: int = -1, num_chunks: int = 0, profile: bool = False, blocks_per_sm: int = 0,
                      initial_guesses: Optional[torch.Tensor] = None,
-                     initial_guesses_offsets: Optional[torch.Tensor] = None):
-    """Build and return ``((adjacency, offsets, status), counters)``; counters as in ``STAT_NAMES``."""
+                     initial_guesses_offsets: Optional[torch.Tensor] = None, diagnostics: bool = False,
+                     model: Optional[torch.Tensor] = None):
+    """Build and return ``((adjacency, offsets, status), counters)``; counters as in ``STAT_NAMES``.
+
+    With ``diagnostics=True`` the counters also hold ``radius`` (float32 [N], the certified radius
+    of each final cell) and ``work`` (int32 [N, 4]: BVH nodes visited, leaves visited, candidates
+    tested, peak node-queue length). ``model`` is a packed learned-radius model (uint8 tensor).
+    """
     if weights is not None and weights.dim() == 1:
         weights = weights[:, None]
     res = _run(points, weights, knn, False, initial_guesses, initial_guesses_offsets, leaf_size,
-               num_chunks=num_chunks, stats=True, profile=profile, blocks_per_sm=blocks_per_sm)
-    return res, dict(_last_stats)
+               num_chunks=num_chunks, stats=True, profile=profile, blocks_per_sm=blocks_per_sm,
+               diagnostics=diagnostics, model=model)
+    out = dict(_last_stats)
+    out.update(_last_diag)
+    return res, out
 
 
 __all__ = ["build_laguerre_voronoi_ultra", "build_voronoi_ultra", "build_with_stats", "last_profile", "STAT_NAMES",

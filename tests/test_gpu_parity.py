@@ -208,3 +208,56 @@ def test_empty_input(dev):
 
     d = pg.voronoi_diagram(torch.zeros(0, 3, device=dev))
     assert d.adjacency.numel() == 0 and d.offsets.tolist() == [0] and d.status.numel() == 0
+
+
+def _lattice_block(m, lo, k, seed):
+    """k^3 points of the jittered m^3 lattice (spacing 1/m, jitter +-1e-4 spacing) and its weights."""
+    rng = np.random.default_rng(seed)
+    s = 1.0 / m
+    idx = np.arange(lo, lo + k, dtype=np.float64)
+    g = np.stack(np.meshgrid(idx, idx, idx, indexing="ij"), -1).reshape(-1, 3)
+    pts = ((g + 0.5) * s + rng.uniform(-1e-4 * s, 1e-4 * s, size=g.shape)).astype(np.float32)
+    w = (rng.random(len(g)) * 0.1 * s * s).astype(np.float32)
+    return pts, w
+
+
+def test_lattice_hull_cells_stay_local(dev, oracle):
+    """Hull cells of a 1/310-spaced jittered lattice are prisms reaching the box 1.0 away, with
+    nearly dependent plane triples along their edges. Exact results, and the traversal of those
+    cells stays local (their empty spheres are not inflated by FP32 vertex error)."""
+    import paragram_b200.cuda as pc
+
+    pts, w = _lattice_block(310, 120, 24, seed=11)
+    for wt in (w, None):
+        t = torch.from_numpy(pts).to(dev)
+        tw = None if wt is None else torch.from_numpy(wt).to(dev)
+        (a, o, s), st = pc.build_with_stats(t, tw, diagnostics=True)
+        _assert_same((a.cpu().numpy(), o.cpu().numpy(), s.cpu().numpy()), oracle.diagram(pts, wt), "lattice block")
+        work = st["work"].cpu().numpy()
+        g = np.round(pts * 310 - 0.5).astype(np.int64) - 120
+        hull = (np.minimum(g, 23 - g).min(1) == 0)
+        assert hull.sum() > 0
+        assert work[hull, 0].mean() < 400, work[hull].mean(0)   # BVH nodes per hull cell
+        assert work[:, 3].max() < 256                          # node queue never near its capacity
+
+
+def test_diagnostics(dev, oracle):
+    """Per-cell certified radius and work counters: a face of the final cell lies within the
+    radius, so every neighbour q satisfies |q - s| / 2 <= R for Voronoi."""
+    import paragram_b200.cuda as pc
+    from paragram_b200 import workloads as W
+
+    pts = W.clustered(30000, seed=8)
+    (a, o, s), st = pc.build_with_stats(torch.from_numpy(pts).to(dev), diagnostics=True)
+    a, o = a.cpu().numpy(), o.cpu().numpy()
+    R = st["radius"].cpu().numpy()
+    work = st["work"].cpu().numpy()
+    assert R.shape == (len(pts),) and work.shape == (len(pts), 4)
+    assert (R > 0).all()
+    src = np.repeat(np.arange(len(pts)), np.diff(o))
+    half = 0.5 * np.linalg.norm(pts[a].astype(np.float64) - pts[src], axis=1)
+    assert (half <= R[src].astype(np.float64) * (1 + 1e-5)).all()
+    assert (work >= 0).all() and (work[:, 0] >= 1).all()
+    assert (work[:, 2] >= np.diff(o)).all()  # every face neighbour was a tested candidate
+    # deferred cells are counted twice in the totals (fast pass, then the 256-slot pass)
+    assert int(work[:, 0].sum()) <= st["nodes"] and int(work[:, 1].sum()) <= st["leaves"]
