@@ -65,6 +65,10 @@ typedef struct pg_options
     int32_t reserved;      /* must be 0 */
     const void *model;     /* learned search radius: device pointer to a pg_model, or NULL for the
                               plain traversal. No reference counterpart. Results do not depend on it. */
+    const float *radius_hint; /* device float32 [num_points] or NULL: a search radius per point (for
+                              instance the radius_out of a previous build of slightly moved points).
+                              Used like the model's prediction; ignored when model is set. Results
+                              do not depend on it. */
     float *radius_out;     /* device float32 [num_points] or NULL: per point, the certified radius of its
                               final cell (max distance of a vertex from the point, power-adjusted;
                               0 for an empty cell). Training targets of the learned radius. */

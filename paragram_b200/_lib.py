@@ -24,6 +24,7 @@ class PgOptions(ctypes.Structure):
         ("blocks_per_sm", ctypes.c_int32),
         ("reserved", ctypes.c_int32),
         ("model", ctypes.c_void_p),
+        ("radius_hint", ctypes.c_void_p),
         ("radius_out", ctypes.c_void_p),
         ("work_out", ctypes.c_void_p),
     ]

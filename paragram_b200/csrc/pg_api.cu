@@ -73,6 +73,7 @@ size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
     w.flags = (int *)take(4 * N);
     w.nbox = (float4 *)take(32 * N);
     w.records = (float4 *)take(64 * N);
+    w.hint = (float *)take(4 * N);
     w.rows = (int *)take(4 * N * kRowWidth);
     w.deg = (int *)take(4 * N);
     w.big_list = (int *)take(4 * N);
@@ -144,6 +145,14 @@ __global__ void k_single_cloud(int *off, int n)
     off[1] = n;
 }
 
+// search radius per sorted slot from the caller's per-point radii
+__global__ void k_hint_gather(int64_t n, const int *oid, const float *radius, float *hint)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        hint[i] = radius[oid[i]];
+}
+
 static int check_counters(const int *host, int64_t n)
 {
     if (host[2] == 1)
@@ -166,7 +175,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
 {
     g_last_error.clear();
     cudaStream_t st = (cudaStream_t)stream;
-    pg_options opt = {8, -1, 0, 0, 0, 0, nullptr, nullptr, nullptr};
+    pg_options opt = {8, -1, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr};
     if (options)
         opt = *options;
     const bool sync = num_edges != nullptr;
@@ -184,6 +193,8 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         return fail(PG_ERR_INVALID, "leaf_size must be at most 32");
     if (opt.reserved != 0)
         return fail(PG_ERR_INVALID, "options.reserved must be 0");
+    if (opt.model != nullptr)
+        return fail(PG_ERR_INVALID, "options.model: no learned model support in this library");
     if (((uintptr_t)opt.work_out & 15u) != 0 || ((uintptr_t)opt.radius_out & 3u) != 0)
         return fail(PG_ERR_INVALID, "work_out must be 16-byte and radius_out 4-byte aligned");
     size_t need = workspace_layout(n, num_clouds, nullptr, nullptr);
@@ -248,6 +259,13 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     }
     cl.radius_out = opt.radius_out;
     cl.work_out = opt.work_out;
+    cl.use_hint = 0;
+    if (opt.radius_hint != nullptr)
+    {
+        ++g_launches;
+        k_hint_gather<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, ws.oid, opt.radius_hint, ws.hint);
+        cl.use_hint = 1;
+    }
     int chunks = sync ? plan_chunks(n, opt.num_chunks) : std::max(opt.num_chunks, 1);
     int sms = device_sms();
     int64_t per = (n + chunks - 1) / chunks;

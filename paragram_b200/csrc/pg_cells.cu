@@ -94,6 +94,7 @@ struct CellArgs
     int inline_big; // rebuild deferred cells right away in the same kernel (warp path)
     float *radius_out; // optional per-cell diagnostics (original ids)
     int4 *work_out;
+    const float *hint; // search radius per sorted slot (learned or given), or nullptr
 };
 
 enum Flag : int
@@ -928,7 +929,134 @@ __device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP
     return run_batch(m, ws, have, q, qkey, A, lane, vm, true);
 }
 
-template <int CAP, int STACK, bool GUESS>
+// Best-first BVH traversal of one cell. A pending entry is (parent << 1 | side)
+// with a lower bound of the bisector distance of the child's points; the
+// entry with the smallest bound is popped, dropped if the bound exceeds the
+// radius of the (since shrunk) cell or `cap`, else its box is tested against
+// every vertex's empty sphere and, for a leaf, only the vertices that pass are
+// pre-tested. `capped` reports whether the cap alone dropped a node; leaves
+// whose bound is <= done_cap are skipped (clipped by an earlier pass). Returns
+// false when the cell finished early (emptied or deferred).
+template <int CAP, int STACK, bool GUESS, bool HINT>
+__device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int i, const CellArgs &A, int lane,
+                                         float cap, float done_cap, bool &capped)
+{
+    const float4 *rec = A.rec;
+    if (lane == 0)
+    {
+        m.stk[0] = ws.root << 1;
+        m.skey[0] = 0.0f;
+        m.stk[1] = (ws.root << 1) | 1;
+        m.skey[1] = 0.0f;
+    }
+    int sp = 2;
+    __syncwarp();
+    while (sp > 0)
+    {
+        PG_T0(tn);
+        int jb = sp - 1;
+        if (sp <= STACK - 64)
+        {
+            unsigned best = 0xFFFFFFFFu;
+            for (int j = lane; j < sp; j += 32)
+                best = min(best, (__float_as_uint(m.skey[j]) & ~(unsigned)(STACK - 1)) | (unsigned)j);
+            best = __reduce_min_sync(kFull, best);
+            jb = (int)(best & (unsigned)(STACK - 1));
+        }
+        // else: a nearly full queue continues depth first (newest entry), which adds at most one
+        // pending entry per tree level; the order of visits never changes the cell.
+        int ent = m.stk[jb];
+        float key = m.skey[jb];
+        __syncwarp();
+        if (lane == 0)
+        {
+            m.stk[jb] = m.stk[sp - 1];
+            m.skey[jb] = m.skey[sp - 1];
+        }
+        --sp;
+        __syncwarp();
+        if (key > ws.rsafe)
+        {
+            PG_T1(m, lane, kStatCycNodes, tn);
+            continue;
+        }
+        if (HINT && key > cap)
+        {
+            capped = true;
+            continue;
+        }
+        PG_COUNT(m, lane, kStatNodes, 1);
+        int parent = ent >> 1, side = ent & 1;
+        const float4 *r = rec + 4 * (size_t)parent;
+        float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+        float lx, ly, lz, hx, hy, hz, mw;
+        int ref;
+        if (side == 0)
+        {
+            lx = r0.x; ly = r0.y; lz = r0.z; hx = r0.w; hy = r1.x; hz = r1.y; mw = r3.z;
+            ref = __float_as_int(r3.x);
+        }
+        else
+        {
+            lx = r1.z; ly = r1.w; lz = r2.x; hx = r2.y; hy = r2.z; hz = r2.w; mw = r3.w;
+            ref = __float_as_int(r3.y);
+        }
+        if (HINT && ref_is_leaf(ref) && !(key > done_cap))
+            continue; // clipped by the first pass
+        VMask<CAP / 32> vm;
+        bool any = node_vertex_mask(m, ws, lx, ly, lz, hx, hy, hz, mw, lane, vm);
+        PG_T1(m, lane, kStatCycNodes, tn);
+        if (!any)
+            continue;
+        if (ref_is_leaf(ref))
+        {
+            PG_T0(tl);
+            bool go = leaf_batch<CAP, STACK, GUESS>(m, ws, ref, i, A, lane, vm);
+            PG_T1(m, lane, kStatCycLeaves, tl);
+            if (!go)
+                return false;
+            continue;
+        }
+        PG_T0(tn2);
+        // internal: queue both children with their distance bounds
+        const float4 *rc = rec + 4 * (size_t)ref;
+        float4 c0 = rc[0], c1 = rc[1], c2 = rc[2], c3 = rc[3];
+        float k0, k1;
+        bool p0 = box_key(ws, c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c3.z, k0);
+        bool p1 = box_key(ws, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w, c3.w, k1);
+        if (HINT)
+        {
+            capped = capped || (p0 && k0 > cap) || (p1 && k1 > cap);
+            p0 = p0 && !(k0 > cap);
+            p1 = p1 && !(k1 > cap);
+        }
+        if (sp + 2 > STACK)
+        {
+            ws.flags |= kFlagDefer;
+            PG_COUNT(m, lane, kStatDeferStack, 1);
+            return false;
+        }
+        if (lane == 0)
+        {
+            if (p0)
+            {
+                m.stk[sp] = ref << 1;
+                m.skey[sp] = k0;
+            }
+            if (p1)
+            {
+                m.stk[sp + (p0 ? 1 : 0)] = (ref << 1) | 1;
+                m.skey[sp + (p0 ? 1 : 0)] = k1;
+            }
+        }
+        sp += (p0 ? 1 : 0) + (p1 ? 1 : 0);
+        ws.peak = max(ws.peak, sp);
+        __syncwarp();
+        PG_T1(m, lane, kStatCycNodes, tn2);
+    }    return true;
+}
+
+template <int CAP, int STACK, bool GUESS, bool HINT>
 __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int i, const CellArgs &A, int lane)
 {
     ws.s = A.pts[i];
@@ -1001,125 +1129,45 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
             return;
     }
     PG_T1(m, lane, kStatCycWarm, tw);
-    // 2. BVH traversal, best first. A pending entry is (parent << 1 | side) with
-    // a lower bound of the bisector distance of the child's points; the entry
-    // with the smallest bound is popped, dropped if the bound exceeds the radius
-    // of the (since shrunk) cell, else its box is tested against every vertex's
-    // empty sphere and, for a leaf, only the vertices that pass are pre-tested.
-    const float4 *rec = A.rec;
-    int sp = 0;
+    // 2. BVH traversal, best first (traverse). With a search radius (learned or
+    // given), the first pass also drops every node whose bound exceeds it; if
+    // the final radius of the cell is within it, the dropped nodes could not
+    // clip the cell (certificate), else a second, unbounded pass follows and
+    // skips the leaves already clipped.
     if (ref_is_leaf(ws.root))
     {
         VMask<CAP / 32> allv;
 #pragma unroll
         for (int k = 0; k < CAP / 32; ++k)
             allv.w[k] = 0xFFFFFFFFu;
-        if (!leaf_batch<CAP, STACK, GUESS>(m, ws, ws.root, i, A, lane, allv))
+        leaf_batch<CAP, STACK, GUESS>(m, ws, ws.root, i, A, lane, allv);
+        return;
+    }
+    float cap = INFINITY, done_cap = -1.0f;
+    if (HINT && A.hint != nullptr)
+    {
+        float rq = A.hint[i];
+        if (rq > 0.0f && rq < 1e30f)
+            cap = rq;
+    }
+    for (int pass = 0; pass < 2; ++pass)
+    {
+        bool capped = false;
+        if (!traverse<CAP, STACK, GUESS, HINT>(m, ws, i, A, lane, cap, done_cap, capped))
             return;
-    }
-    else
-    {
-        if (lane == 0)
+        if (!HINT || !capped)
+            return;
+        if (ws.rsafe <= cap)
         {
-            m.stk[0] = ws.root << 1;
-            m.skey[0] = 0.0f;
-            m.stk[1] = (ws.root << 1) | 1;
-            m.skey[1] = 0.0f;
-        }
-        sp = 2;
-    }
-    __syncwarp();
-    while (sp > 0)
-    {
-        PG_T0(tn);
-        int jb = sp - 1;
-        if (sp <= STACK - 64)
-        {
-            unsigned best = 0xFFFFFFFFu;
-            for (int j = lane; j < sp; j += 32)
-                best = min(best, (__float_as_uint(m.skey[j]) & ~(unsigned)(STACK - 1)) | (unsigned)j);
-            best = __reduce_min_sync(kFull, best);
-            jb = (int)(best & (unsigned)(STACK - 1));
-        }
-        // else: a nearly full queue continues depth first (newest entry), which adds at most one
-        // pending entry per tree level; the order of visits never changes the cell.
-        int ent = m.stk[jb];
-        float key = m.skey[jb];
-        __syncwarp();
-        if (lane == 0)
-        {
-            m.stk[jb] = m.stk[sp - 1];
-            m.skey[jb] = m.skey[sp - 1];
-        }
-        --sp;
-        __syncwarp();
-        if (key > ws.rsafe)
-        {
-            PG_T1(m, lane, kStatCycNodes, tn);
-            continue;
-        }
-        PG_COUNT(m, lane, kStatNodes, 1);
-        int parent = ent >> 1, side = ent & 1;
-        const float4 *r = rec + 4 * (size_t)parent;
-        float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
-        float lx, ly, lz, hx, hy, hz, mw;
-        int ref;
-        if (side == 0)
-        {
-            lx = r0.x; ly = r0.y; lz = r0.z; hx = r0.w; hy = r1.x; hz = r1.y; mw = r3.z;
-            ref = __float_as_int(r3.x);
-        }
-        else
-        {
-            lx = r1.z; ly = r1.w; lz = r2.x; hx = r2.y; hy = r2.z; hz = r2.w; mw = r3.w;
-            ref = __float_as_int(r3.y);
-        }
-        VMask<CAP / 32> vm;
-        bool any = node_vertex_mask(m, ws, lx, ly, lz, hx, hy, hz, mw, lane, vm);
-        PG_T1(m, lane, kStatCycNodes, tn);
-        if (!any)
-            continue;
-        if (ref_is_leaf(ref))
-        {
-            PG_T0(tl);
-            bool go = leaf_batch<CAP, STACK, GUESS>(m, ws, ref, i, A, lane, vm);
-            PG_T1(m, lane, kStatCycLeaves, tl);
-            if (!go)
-                return;
-            continue;
-        }
-        PG_T0(tn2);
-        // internal: queue both children with their distance bounds
-        const float4 *rc = rec + 4 * (size_t)ref;
-        float4 c0 = rc[0], c1 = rc[1], c2 = rc[2], c3 = rc[3];
-        float k0, k1;
-        bool p0 = box_key(ws, c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c3.z, k0);
-        bool p1 = box_key(ws, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w, c3.w, k1);
-        if (sp + 2 > STACK)
-        {
-            ws.flags |= kFlagDefer;
-            PG_COUNT(m, lane, kStatDeferStack, 1);
+            PG_COUNT(m, lane, kStatHintHit, 1);
             return;
         }
-        if (lane == 0)
-        {
-            if (p0)
-            {
-                m.stk[sp] = ref << 1;
-                m.skey[sp] = k0;
-            }
-            if (p1)
-            {
-                m.stk[sp + (p0 ? 1 : 0)] = (ref << 1) | 1;
-                m.skey[sp + (p0 ? 1 : 0)] = k1;
-            }
-        }
-        sp += (p0 ? 1 : 0) + (p1 ? 1 : 0);
-        ws.peak = max(ws.peak, sp);
-        __syncwarp();
-        PG_T1(m, lane, kStatCycNodes, tn2);
+        PG_COUNT(m, lane, kStatHintMiss, 1);
+        done_cap = cap;
+        cap = INFINITY;
     }
 }
+
 
 // Optional per-cell diagnostics: certified radius and traversal work.
 template <int CAP, int STACK>
@@ -1158,7 +1206,7 @@ template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, i
         slot = atomicAdd(&A.counters[1], 1);
     slot = __shfl_sync(kFull, slot, 0);
     __syncwarp();
-    process_cell<kCapBig, kStackBig, GUESS>(m, ws, i, A, lane);
+    process_cell<kCapBig, kStackBig, GUESS, false>(m, ws, i, A, lane);
     write_diagnostics(m, ws, A, lane);
     if ((ws.flags & kFlagError) && lane == 0)
         atomicExch(&A.counters[2], 1);
@@ -1176,7 +1224,7 @@ template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, i
     flush_stats(m, A, lane);
 }
 
-template <int CAP, int STACK, bool GUESS>
+template <int CAP, int STACK, bool GUESS, bool HINT>
 __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArgs &A, int lane)
 {
     WarpState<CAP> ws;
@@ -1195,7 +1243,7 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
             break;
         int i = A.big_pass ? A.big_list[t] : (int)(A.begin + t);
         PG_T0(tcell);
-        process_cell<CAP, STACK, GUESS>(m, ws, i, A, lane);
+        process_cell<CAP, STACK, GUESS, HINT>(m, ws, i, A, lane);
         write_diagnostics(m, ws, A, lane);
         if (A.big_pass)
             ws.si = t; // the deferred-row slot
@@ -1235,12 +1283,12 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
     flush_stats(m, A, lane);
 }
 
-template <int MINB, bool GUESS>
+template <int MINB, bool GUESS, bool HINT>
 __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) k_cells_fast(CellArgs A)
 {
     __shared__ CellMem<kCapFast, kStackFast> mem[kWarpsPerBlock];
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    cells_body<kCapFast, kStackFast, GUESS>(mem[w], A, lane);
+    cells_body<kCapFast, kStackFast, GUESS, HINT>(mem[w], A, lane);
 }
 
 template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_cells_big(CellArgs A)
@@ -1248,7 +1296,7 @@ template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_c
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     size_t gw = (size_t)blockIdx.x * kWarpsPerBlock + w;
     auto *m = reinterpret_cast<CellMem<kCapBig, kStackBig> *>(A.slabs + gw * sizeof(CellMem<kCapBig, kStackBig>));
-    cells_body<kCapBig, kStackBig, GUESS>(*m, A, lane);
+    cells_body<kCapBig, kStackBig, GUESS, false>(*m, A, lane);
 }
 
 // ===========================================================================
@@ -1789,6 +1837,7 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.inline_big = 0;
     A.radius_out = cl.radius_out;
     A.work_out = reinterpret_cast<int4 *>(cl.work_out);
+    A.hint = cl.use_hint ? ws.hint : nullptr;
     return A;
 }
 
@@ -1813,8 +1862,15 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
         k_tcells<<<(unsigned)grid, 256, 0, st>>>(A, (TSlab *)ws.tslabs);
         return;
     }
-    void (*kern)(CellArgs) = cl.guesses ? k_cells_fast<2, true>
-                                        : (cl.min_blocks == 3 ? k_cells_fast<3, false> : k_cells_fast<2, false>);
+    // variants: register budget (2 or 3 blocks per SM), initial guesses, search radius per cell
+    // (a search radius is not used together with initial guesses)
+    void (*kern)(CellArgs);
+    if (cl.guesses)
+        kern = k_cells_fast<2, true, false>;
+    else if (cl.use_hint)
+        kern = cl.min_blocks == 3 ? k_cells_fast<3, false, true> : k_cells_fast<2, false, true>;
+    else
+        kern = cl.min_blocks == 3 ? k_cells_fast<3, false, false> : k_cells_fast<2, false, false>;
     int blocks_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerBlock * 32, 0);
     if (blocks_per_sm < 1)

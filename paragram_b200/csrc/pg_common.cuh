@@ -54,7 +54,9 @@ enum Stat : int
     kStatDeferVerts = 14,  // deferrals / large-pass overflows: vertex or plane slots
     kStatDeferStack = 15,  // deferrals / large-pass overflows: traversal stack
     kStatVertex64 = 16,    // vertices rebuilt in FP64 (ill-conditioned in FP32)
-    kNumStats = 17,
+    kStatHintHit = 17,     // cells certified within their search radius after the radius dropped a node
+    kStatHintMiss = 18,    // cells whose search radius was too small (a second, unbounded pass ran)
+    kNumStats = 19,
 };
 
 // leaf reference encoding in BVH records: bit 31 set, count-1 in bits 26..30,
@@ -121,6 +123,7 @@ struct Workspace
     int *flags;           // [N] refit arrival counters
     float4 *nbox;         // [2N] internal node box lo(xyz)+maxw, hi(xyz)+count
     float4 *records;      // [4N] traversal records of internal nodes
+    float *hint;          // [N] search radius per sorted slot (learned or given), <= 0: none
     // cells
     int *rows;            // [N * kRowWidth] directed rows by original index
     int *deg;             // [N] directed degree by original index (kBigFlag: deferred row)

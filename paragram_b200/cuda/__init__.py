@@ -23,7 +23,7 @@ _LIB = _lib.load()
 #: Counter names returned by ``last_stats()`` (pg_stats in include/paragram_b200.h).
 STAT_NAMES = ["tests", "fp64_escalations", "exact_escalations", "deferred_cells", "nodes", "leaves", "clips",
               "candidates", "cyc_cell", "cyc_warm", "cyc_nodes", "cyc_leaves", "cyc_clips", "cyc_out", "defer_slots",
-              "defer_stack", "vertex64"]
+              "defer_stack", "vertex64", "hint_hits", "hint_misses"]
 _last_stats: dict = {}
 _last_diag: dict = {}
 #: Names of the values returned by ``last_profile()`` (pg_last_profile in include/paragram_b200.h).
@@ -38,7 +38,8 @@ def _check(ok: bool, msg: str):
 def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug: bool,
          initial_guesses: Optional[torch.Tensor], initial_guesses_offsets: Optional[torch.Tensor], leaf_size: int,
          num_chunks: int = 0, stats: bool = False, profile: bool = False, blocks_per_sm: int = 0,
-         diagnostics: bool = False, model: Optional[torch.Tensor] = None):
+         diagnostics: bool = False, model: Optional[torch.Tensor] = None,
+         radius_hint: Optional[torch.Tensor] = None):
     n = int(points.shape[0])
     _check(points.device.type == "cuda", "points must be on CUDA device")
     _check(points.dtype == torch.float32, "points must be of type float")
@@ -69,6 +70,11 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
         _check(model.device == dev and model.dtype == torch.uint8 and model.is_contiguous(),
                "model must be a contiguous uint8 tensor (a packed pg_model) on the points' device")
         opts.model = model.data_ptr()
+    if radius_hint is not None:
+        _check(radius_hint.device == dev and radius_hint.dtype == torch.float32 and radius_hint.numel() == n,
+               "radius_hint must be float32 with one entry per point, on the points' device")
+        radius_hint = radius_hint.contiguous()
+        opts.radius_hint = radius_hint.data_ptr() if n > 0 else None
     radius = work = None
     if diagnostics:
         radius = torch.zeros(max(n, 1), dtype=torch.float32, device=dev)
@@ -129,18 +135,19 @@ def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = Non
                      leaf_size: int = -1, num_chunks: int = 0, profile: bool = False, blocks_per_sm: int = 0,
                      initial_guesses: Optional[torch.Tensor] = None,
                      initial_guesses_offsets: Optional[torch.Tensor] = None, diagnostics: bool = False,
-                     model: Optional[torch.Tensor] = None):
+                     model: Optional[torch.Tensor] = None, radius_hint: Optional[torch.Tensor] = None):
     """Build and return ``((adjacency, offsets, status), counters)``; counters as in ``STAT_NAMES``.
 
     With ``diagnostics=True`` the counters also hold ``radius`` (float32 [N], the certified radius
     of each final cell) and ``work`` (int32 [N, 4]: BVH nodes visited, leaves visited, candidates
-    tested, peak node-queue length). ``model`` is a packed learned-radius model (uint8 tensor).
+    tested, peak node-queue length). ``model`` is a packed learned-radius model (uint8 tensor);
+    ``radius_hint`` (float32 [N]) gives a search radius per point instead.
     """
     if weights is not None and weights.dim() == 1:
         weights = weights[:, None]
     res = _run(points, weights, knn, False, initial_guesses, initial_guesses_offsets, leaf_size,
                num_chunks=num_chunks, stats=True, profile=profile, blocks_per_sm=blocks_per_sm,
-               diagnostics=diagnostics, model=model)
+               diagnostics=diagnostics, model=model, radius_hint=radius_hint)
     out = dict(_last_stats)
     out.update(_last_diag)
     return res, out

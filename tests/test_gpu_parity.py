@@ -261,3 +261,26 @@ def test_diagnostics(dev, oracle):
     assert (work[:, 2] >= np.diff(o)).all()  # every face neighbour was a tested candidate
     # deferred cells are counted twice in the totals (fast pass, then the 256-slot pass)
     assert int(work[:, 0].sum()) <= st["nodes"] and int(work[:, 1].sum()) <= st["leaves"]
+
+
+@pytest.mark.parametrize("scale", [1.001, 0.5, 3.0, 0.0, -1.0, float("nan")])
+def test_radius_hint_never_changes_results(dev, oracle, scale):
+    """A search radius per cell (about right, too small, too large, absent or invalid) changes
+    the work, never the diagram: the capped pass is certified, else an unbounded pass completes it."""
+    import paragram_b200.cuda as pc
+    from paragram_b200 import workloads as W
+
+    for pts, w in ((W.clustered(20000, seed=12), None), W.power_uniform(8000, seed=13)):
+        t = torch.from_numpy(pts).to(dev)
+        tw = None if w is None else torch.from_numpy(w).to(dev)
+        (a, o, s), st = pc.build_with_stats(t, tw, diagnostics=True)
+        hint = st["radius"] * scale
+        (a2, o2, s2), st2 = pc.build_with_stats(t, tw, radius_hint=hint)
+        assert torch.equal(a, a2) and torch.equal(o, o2) and torch.equal(s, s2)
+        _assert_same((a2.cpu().numpy(), o2.cpu().numpy(), s2.cpu().numpy()), oracle.diagram(pts, w), f"hint x{scale}")
+        if scale > 1.0:
+            assert st2["hint_misses"] <= 0.01 * len(pts)
+        if scale == 0.5:
+            assert st2["hint_misses"] > 0.5 * len(pts)
+        if not scale > 0.0:
+            assert st2["hint_hits"] + st2["hint_misses"] == 0
