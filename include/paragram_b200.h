@@ -74,7 +74,41 @@ typedef struct pg_options
                               0 for an empty cell). Training targets of the learned radius. */
     int32_t *work_out;     /* device int32 [4 * num_points] or NULL: per point, BVH nodes visited, leaves
                               visited, candidates tested and the peak length of the node queue. */
+    float *features_out;   /* device float32 [16 * num_points] or NULL: per point, the 16 features of
+                              the learned search radius (training inputs; pg_model below). */
+    int32_t *order_out;    /* device int32 [num_points] or NULL: the points' curve order (sorted slot
+                              -> point index) used by the BVH and by the features' windows. */
 } pg_options;
+
+/* Learned search radius (no reference counterpart). A 16 -> 64 -> 64 -> 2 MLP
+ * with BF16 weights: features of a point (its curve-order window, see
+ * features_out) -> (log of its cell's certified radius relative to the
+ * window's mean neighbour distance, neighbour count / 16), both normalised as
+ * (t - target_mean) * target_scale. A build given a model predicts every
+ * point's radius (times exp(radius_margin)) and caps its first traversal pass
+ * with it; the cap is kept only when the final radius is within it, so the
+ * diagram never depends on the model. Device memory, pg_mlp_model_bytes()
+ * bytes, magic = PG_MODEL_MAGIC, w3 rows 2..7 zero. */
+#define PG_MODEL_MAGIC 0x314D4750u /* "PGM1" */
+typedef struct pg_model
+{
+    uint32_t magic;
+    uint32_t num_features; /* 16 */
+    uint32_t hidden;       /* 64 */
+    uint32_t reserved;
+    float feat_mean[16];   /* inputs are (x - feat_mean) * feat_scale, rounded to BF16 */
+    float feat_scale[16];
+    float target_mean[2];
+    float target_scale[2];
+    float radius_margin;   /* added to the predicted log radius */
+    float pad[3];
+    float b1[64];
+    float b2[64];
+    float b3[8];           /* entries 2..7 unused */
+    uint16_t w1[64 * 16];  /* BF16 bits, [out][in] */
+    uint16_t w2[64 * 64];
+    uint16_t w3[8 * 64];   /* rows 2..7 zero */
+} pg_model;
 
 /* Library version (major * 10000 + minor * 100 + patch). */
 int pg_version(void);
@@ -143,6 +177,26 @@ int pg_build_batch(int64_t total_points, int32_t num_clouds, const int32_t *clou
                    const float *weights, const pg_options *options, void *workspace, size_t workspace_bytes,
                    int32_t *offsets, int32_t *status, int64_t *num_edges, void *stream);
 int pg_batch_check(const void *workspace, int64_t total_points, int32_t num_clouds, void *stream);
+
+/* Training and evaluation kernels of the learned search radius (no reference
+ * counterpart). Parameters: a flat float32 vector of pg_mlp_num_params()
+ * master weights in the order w1 [64][16], b1 [64], w2 [64][64], b2 [64],
+ * w3 [2][64], b3 [2]; the model holds their BF16 / FP32 copies.
+ *   pg_mlp_forward  out [n][2] = network(features [n][16])
+ *   pg_mlp_grad     adds to grad [num_params] the gradient of
+ *                   L = sum_s w_s |y_s - t'_s|^2 * inv_total_weight / 2 (t' = normalised targets [n][2],
+ *                   w = sample_weights [n]) and adds L to *loss (device float); the caller zeroes both
+ *   pg_mlp_adam     one Adam step of params (m, v: moments, step >= 1), then writes the model's weights
+ *   pg_mlp_pack     writes the model's weights from params
+ * All pointers are device pointers; calls are ordered on `stream`. */
+int pg_mlp_num_params(void);
+size_t pg_mlp_model_bytes(void);
+int pg_mlp_forward(int64_t n, const float *features, const void *model, float *out, void *stream);
+int pg_mlp_grad(int64_t n, const float *features, const float *targets, const float *sample_weights,
+                float inv_total_weight, const void *model, float *grad, float *loss, void *stream);
+int pg_mlp_adam(float *params, const float *grad, float *m, float *v, int64_t step, float lr, float beta1,
+                float beta2, float eps, void *model, void *stream);
+int pg_mlp_pack(const float *params, void *model, void *stream);
 
 /* CSR offsets from per-row degrees, allocating nothing. No counterpart in the
  * reference: it is for callers that cannot allocate device memory when they

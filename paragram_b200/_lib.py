@@ -27,13 +27,16 @@ class PgOptions(ctypes.Structure):
         ("radius_hint", ctypes.c_void_p),
         ("radius_out", ctypes.c_void_p),
         ("work_out", ctypes.c_void_p),
+        ("features_out", ctypes.c_void_p),
+        ("order_out", ctypes.c_void_p),
     ]
 
 
 #: Symbols declared in include/paragram_b200.h.
 EXPORTED = ["pg_version", "pg_last_error", "pg_workspace_size", "pg_build", "pg_emit_adjacency", "pg_stats",
             "pg_last_profile", "pg_degrees_to_offsets_noalloc", "pg_batch_workspace_size", "pg_build_batch",
-            "pg_batch_check"]
+            "pg_batch_check", "pg_mlp_num_params", "pg_mlp_model_bytes", "pg_mlp_forward", "pg_mlp_grad",
+            "pg_mlp_adam", "pg_mlp_pack"]
 
 
 def load() -> ctypes.CDLL:
@@ -69,6 +72,17 @@ def load() -> ctypes.CDLL:
         lib.pg_build_batch.restype = ctypes.c_int
         lib.pg_batch_check.argtypes = [vp, i64, i32, vp]
         lib.pg_batch_check.restype = ctypes.c_int
+        lib.pg_mlp_num_params.restype = ctypes.c_int
+        lib.pg_mlp_model_bytes.restype = sz
+        lib.pg_mlp_forward.argtypes = [i64, vp, vp, vp, vp]
+        lib.pg_mlp_forward.restype = ctypes.c_int
+        lib.pg_mlp_grad.argtypes = [i64, vp, vp, vp, ctypes.c_float, vp, vp, vp, vp]
+        lib.pg_mlp_grad.restype = ctypes.c_int
+        lib.pg_mlp_adam.argtypes = [vp, vp, vp, vp, i64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_float, vp, vp]
+        lib.pg_mlp_adam.restype = ctypes.c_int
+        lib.pg_mlp_pack.argtypes = [vp, vp, vp]
+        lib.pg_mlp_pack.restype = ctypes.c_int
         lib.pg_degrees_to_offsets_noalloc.argtypes = [i64, vp, vp, vp]
         lib.pg_degrees_to_offsets_noalloc.restype = ctypes.c_int
         _lib = lib

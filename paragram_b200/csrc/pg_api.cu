@@ -175,7 +175,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
 {
     g_last_error.clear();
     cudaStream_t st = (cudaStream_t)stream;
-    pg_options opt = {8, -1, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr};
+    pg_options opt = {8, -1, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (options)
         opt = *options;
     const bool sync = num_edges != nullptr;
@@ -193,8 +193,8 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         return fail(PG_ERR_INVALID, "leaf_size must be at most 32");
     if (opt.reserved != 0)
         return fail(PG_ERR_INVALID, "options.reserved must be 0");
-    if (opt.model != nullptr)
-        return fail(PG_ERR_INVALID, "options.model: no learned model support in this library");
+    if (((uintptr_t)opt.features_out & 15u) != 0 || ((uintptr_t)opt.model & 15u) != 0)
+        return fail(PG_ERR_INVALID, "features_out and model must be 16-byte aligned");
     if (((uintptr_t)opt.work_out & 15u) != 0 || ((uintptr_t)opt.radius_out & 3u) != 0)
         return fail(PG_ERR_INVALID, "work_out must be 16-byte and radius_out 4-byte aligned");
     size_t need = workspace_layout(n, num_clouds, nullptr, nullptr);
@@ -260,7 +260,16 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     cl.radius_out = opt.radius_out;
     cl.work_out = opt.work_out;
     cl.use_hint = 0;
-    if (opt.radius_hint != nullptr)
+    if (opt.features_out != nullptr)
+        features_launch(ws, n, num_clouds, opt.features_out, st);
+    if (opt.order_out != nullptr)
+        cudaMemcpyAsync(opt.order_out, ws.oid, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st);
+    if (opt.model != nullptr)
+    {
+        predict_launch(ws, n, num_clouds, (const pg_model *)opt.model, st);
+        cl.use_hint = 1;
+    }
+    else if (opt.radius_hint != nullptr)
     {
         ++g_launches;
         k_hint_gather<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, ws.oid, opt.radius_hint, ws.hint);

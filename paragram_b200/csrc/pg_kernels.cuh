@@ -1,7 +1,11 @@
 // pg_kernels.cuh -- host-side launchers shared between the translation units.
 #pragma once
 
+#include <string>
+
 #include "pg_common.cuh"
+
+struct pg_model; // include/paragram_b200.h
 
 namespace pg
 {
@@ -37,6 +41,11 @@ struct CellLaunch
 };
 void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int num_sms, cudaStream_t st);
 void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st);
+
+// pg_mlp.cu
+void features_launch(const Workspace &ws, int64_t n, int num_clouds, float *out, cudaStream_t st);
+void predict_launch(const Workspace &ws, int64_t n, int num_clouds, const ::pg_model *model, cudaStream_t st);
+int set_last_error(int code, const std::string &msg);
 
 // pg_csr.cu
 void csr_count(const Workspace &ws, int64_t n, int32_t *offsets, cudaStream_t st);

@@ -39,7 +39,7 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
          initial_guesses: Optional[torch.Tensor], initial_guesses_offsets: Optional[torch.Tensor], leaf_size: int,
          num_chunks: int = 0, stats: bool = False, profile: bool = False, blocks_per_sm: int = 0,
          diagnostics: bool = False, model: Optional[torch.Tensor] = None,
-         radius_hint: Optional[torch.Tensor] = None):
+         radius_hint: Optional[torch.Tensor] = None, features: bool = False):
     n = int(points.shape[0])
     _check(points.device.type == "cuda", "points must be on CUDA device")
     _check(points.dtype == torch.float32, "points must be of type float")
@@ -75,11 +75,15 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
                "radius_hint must be float32 with one entry per point, on the points' device")
         radius_hint = radius_hint.contiguous()
         opts.radius_hint = radius_hint.data_ptr() if n > 0 else None
-    radius = work = None
+    radius = work = feats = order = None
     if diagnostics:
         radius = torch.zeros(max(n, 1), dtype=torch.float32, device=dev)
         work = torch.zeros(max(n, 1), 4, dtype=torch.int32, device=dev)
         opts.radius_out, opts.work_out = radius.data_ptr(), work.data_ptr()
+    if features:
+        feats = torch.zeros(max(n, 1), 16, dtype=torch.float32, device=dev)
+        order = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
+        opts.features_out, opts.order_out = feats.data_ptr(), order.data_ptr()
     with torch.cuda.device(dev):
         nbytes = ctypes.c_size_t(0)
         rc = _LIB.pg_workspace_size(n, ctypes.byref(nbytes))
@@ -107,6 +111,8 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
     _last_diag.clear()
     if diagnostics:
         _last_diag.update(radius=radius[:n], work=work[:n])
+    if features:
+        _last_diag.update(features=feats[:n], order=order[:n])
     return adjacency, offsets, status
 
 
@@ -135,19 +141,22 @@ def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = Non
                      leaf_size: int = -1, num_chunks: int = 0, profile: bool = False, blocks_per_sm: int = 0,
                      initial_guesses: Optional[torch.Tensor] = None,
                      initial_guesses_offsets: Optional[torch.Tensor] = None, diagnostics: bool = False,
-                     model: Optional[torch.Tensor] = None, radius_hint: Optional[torch.Tensor] = None):
+                     model: Optional[torch.Tensor] = None, radius_hint: Optional[torch.Tensor] = None,
+                     features: bool = False):
     """Build and return ``((adjacency, offsets, status), counters)``; counters as in ``STAT_NAMES``.
 
     With ``diagnostics=True`` the counters also hold ``radius`` (float32 [N], the certified radius
     of each final cell) and ``work`` (int32 [N, 4]: BVH nodes visited, leaves visited, candidates
     tested, peak node-queue length). ``model`` is a packed learned-radius model (uint8 tensor);
-    ``radius_hint`` (float32 [N]) gives a search radius per point instead.
+    ``radius_hint`` (float32 [N]) gives a search radius per point instead. With ``features=True``
+    the counters also hold ``features`` (float32 [N, 16], the learned model's inputs) and
+    ``order`` (int32 [N], the curve order: sorted slot -> point index).
     """
     if weights is not None and weights.dim() == 1:
         weights = weights[:, None]
     res = _run(points, weights, knn, False, initial_guesses, initial_guesses_offsets, leaf_size,
                num_chunks=num_chunks, stats=True, profile=profile, blocks_per_sm=blocks_per_sm,
-               diagnostics=diagnostics, model=model, radius_hint=radius_hint)
+               diagnostics=diagnostics, model=model, radius_hint=radius_hint, features=features)
     out = dict(_last_stats)
     out.update(_last_diag)
     return res, out

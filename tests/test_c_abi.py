@@ -21,7 +21,7 @@ def test_header_symbols_exported(lib):
     from paragram_b200 import _lib
 
     header = open(os.path.join(ROOT, "include", "paragram_b200.h")).read()
-    declared = set(re.findall(r"^\s*(?:int|const char \*)\s*(pg_\w+)\s*\(", header, re.M))
+    declared = set(re.findall(r"^\s*(?:int|size_t|const char \*)\s*(pg_\w+)\s*\(", header, re.M))
     assert declared == set(_lib.EXPORTED)
     for name in declared:
         assert hasattr(lib, name), name
@@ -66,3 +66,15 @@ def test_build_rejects_bad_arguments(lib):
 
 def test_emit_rejects_bad_arguments(lib):
     assert lib.pg_emit_adjacency(10, None, None, None, None) == -1
+
+
+def test_mlp_entry_points_without_gpu(lib):
+    """Sizes of the learned-radius model and argument checks (no kernel runs)."""
+    assert lib.pg_mlp_num_params() == 5378
+    assert lib.pg_mlp_model_bytes() == 11984
+    assert lib.pg_mlp_forward(-1, None, None, None, None) == -1
+    assert lib.pg_mlp_forward(0, None, None, None, None) == 0
+    assert lib.pg_mlp_grad(10, None, None, None, 1.0, None, None, None, None) == -1
+    assert lib.pg_mlp_adam(None, None, None, None, 1, 1e-3, 0.9, 0.999, 1e-8, None, None) == -1
+    assert lib.pg_mlp_adam(256, 256, 256, 256, 0, 1e-3, 0.9, 0.999, 1e-8, 256, None) == -1  # step must be >= 1
+    assert lib.pg_mlp_pack(None, None, None) == -1
