@@ -2,13 +2,20 @@
 
 Default workload (the headline configuration): Voronoi diagram of N = 5,000,000
 clustered points (90% from 64 truncated isotropic Gaussians, sigma log-uniform
-in [0.005, 0.1], 10% uniform background), seeded synthetic data. One step is
-one full ``paragram_b200.voronoi_diagram`` call (LBVH build, cell clipping,
-CSR) on device-resident points; ``e2e`` repeats the step through the same
-public API from pinned host memory, with the host->device copy of the points
-and the device->host copy of the Diagram inside the timed region.
+in [0.005, 0.1], 10% uniform background), seeded synthetic data, built with the
+learned search radius (a model trained before timing on two 1M-point clouds of
+disjoint seeds) and FP32-filtered predicates; the plain build (no model) of the
+same points is timed beside it. One step is one full build (LBVH, prediction,
+cell clipping, CSR, adjacency) on device-resident points; ``e2e`` repeats the
+step through the public API from pinned host memory, with the host->device
+copy of the points and the device->host copy of the Diagram inside the timed
+region.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--workload NAME]
+
+Workloads: clustered_voronoi_5m (default), clustered_voronoi_500k,
+uniform_voronoi_100k, uniform_power_1m, lattice_power_310 (29.8M-point jittered
+lattice, power), surface_batch_256 (256 surface clouds in one CUDA-graph batch).
 
 For N > 1 (torch.distributed.run, one process per GPU) every rank builds its
 own diagram of an equally sized, differently seeded point set (weak scaling;
@@ -44,7 +51,10 @@ WORKLOADS = {
     "uniform_voronoi_100k": dict(kind="uniform", n=100_000, weighted=False),
     "uniform_power_1m": dict(kind="power", n=1_000_000, weighted=True),
     "lattice_power_310": dict(kind="lattice", n=310 ** 3, weighted=True),
+    "surface_batch_256": dict(kind="surfaces", n=256, weighted=False),
 }
+#: workloads built with the learned search radius (plain build timed beside them)
+LEARNED = {"clustered_voronoi_5m", "clustered_voronoi_500k"}
 
 
 def make_points(spec: dict, seed: int):
@@ -59,7 +69,27 @@ def make_points(spec: dict, seed: int):
         return W.power_uniform(spec["n"], seed=seed)
     if k == "lattice":
         return W.jittered_lattice(round(spec["n"] ** (1 / 3)), seed=seed)
+    if k == "surfaces":
+        return W.surface_clouds(num_clouds=spec["n"], seed=seed), None
     raise ValueError(k)
+
+
+def train_model(dev, seed: int):
+    """Learned search radius trained on two 1M-point clustered clouds of other seeds (GPU kernels)."""
+    import torch
+
+    from paragram_b200 import learned
+    from paragram_b200 import workloads as W
+
+    t0 = time.perf_counter()
+    data = [learned.collect(torch.from_numpy(W.clustered(1_000_000, seed=1000 + 2 * seed + k)).to(dev))
+            for k in range(2)]
+    log = []
+    model = learned.train(data, epochs=4, batch=8192, log=log)
+    margin = model.calibrate(data[0], quantile=0.98)
+    torch.cuda.synchronize(dev)
+    return model, {"train_s": time.perf_counter() - t0, "train_samples": sum(int(d.weights.sum()) for d in data),
+                   "loss_per_epoch": [round(x, 4) for x in log], "margin": margin, "calibration_quantile": 0.98}
 
 
 class ClockSampler:
@@ -162,19 +192,42 @@ def cpu_oracle_rate(pts, w, sample: int, threads: int = 0) -> dict:
             "tree_s": c.tree_seconds, "cells_s": c.seconds, "wall_s": wall}
 
 
+def cpu_oracle_rate_clouds(clouds, sample: int) -> dict:
+    """Oracle rate over whole clouds taken in order until `sample` cells (each cloud its own diagram)."""
+    from oracle import pg_oracle
+
+    cells, secs, tree, threads, used = 0, 0.0, 0.0, 0, 0
+    t0 = time.perf_counter()
+    for c in clouds:
+        if cells >= sample:
+            break
+        r = pg_oracle.cells(c, None, mode="incremental", threads=0)
+        cells += len(c)
+        secs += r.seconds + r.tree_seconds
+        tree += r.tree_seconds
+        threads = r.threads
+        used += 1
+    return {"value": cells / max(secs, 1e-9) / 1e6, "cores": threads, "cells": cells, "tree_s": tree,
+            "cells_s": secs - tree, "wall_s": time.perf_counter() - t0, "clouds": used}
+
+
 def run_reference(args, spec, rank, world):
     """CPU restatement of the reference's construction on the host cores (rank 0 only)."""
     if rank != 0:
         return
     pts, w = make_points(spec, seed=0)
     sample = args.cpu_sample
+    clouds = spec["kind"] == "surfaces"
+    rate = (lambda m: cpu_oracle_rate_clouds(pts, m)) if clouds else (lambda m: cpu_oracle_rate(pts, w, m))
     for _ in range(args.warmup):
-        cpu_oracle_rate(pts, w, max(sample // 10, 1000))
+        rate(max(sample // 10, 1000))
     vals = []
     info = None
     for _ in range(args.steps):
-        info = cpu_oracle_rate(pts, w, sample)
+        info = rate(sample)
         vals.append(info["value"])
+    if clouds:
+        spec = dict(spec, n=int(sum(len(c) for c in pts)))
     value = statistics.median(vals)
     line = {
         "impl": "reference",
@@ -201,109 +254,161 @@ def run_reference(args, spec, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def _timed(fn, steps, dev, flush):
+    """Run fn `steps` times, L2 flushed before each, timed with CUDA events on the current stream."""
+    import torch
+
+    import paragram_b200.cuda as pc
+
+    times, cell_ms, launches, out = [], [], 0, None
+    for _ in range(steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize(dev)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = fn()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        times.append(e0.elapsed_time(e1))
+        prof = pc.last_profile()
+        cell_ms.append(prof["cells_ms"])
+        launches += int(prof["launches"])
+    return times, cell_ms, launches, out
+
+
+def _peaks():
+    try:
+        return json.load(open(MEASURED_PEAKS))
+    except (OSError, ValueError):
+        return {}
+
+
+def _roofline(flops, nbytes, cell_s, csum, kernel, traffic):
+    peaks = _peaks()
+    peak = fp32_peak_tflops(peaks.get("sm_max_mhz") or csum.get("sm_max_mhz"))
+    achieved = flops / cell_s / 1e12 if cell_s > 0 else None
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    return {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "kernel": kernel, "cell_pass_ms": cell_s * 1e3,
+            "algorithmic_flops": flops, "algorithmic_bytes": nbytes,
+            "hbm_frac": (nbytes / cell_s / 1e9) / hbm_peak if cell_s > 0 else None,
+            "peak_note": "nominal FP32 FMA peak 148 SM x 128 lanes x 2 x max SM clock "
+                         "(MEASURED_PEAKS has no FP32 figure)"}
+
+
+def _cpu_baseline(args, world, pts, w, n):
+    if world != 1 or args.no_cpu_baseline:
+        return None
+    try:
+        cb = cpu_oracle_rate(pts, w, args.cpu_sample)
+        return {"value": cb["value"], "unit": "Mcells/s", "cores": cb["cores"], "kind": "port",
+                "sample": f"{cb['cells']} of {n} cells; kd-tree {cb['tree_s']:.2f} s + cells "
+                          f"{cb['cells_s']:.2f} s on {cb['cores']} threads, extrapolated to all cells"}
+    except Exception as exc:  # the baseline must not hide the GPU number
+        return {"value": None, "unit": "Mcells/s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
+
+
+def _cpu_baseline_clouds(args, world, clouds):
+    if world != 1 or args.no_cpu_baseline:
+        return None
+    try:
+        cb = cpu_oracle_rate_clouds(clouds, args.cpu_sample)
+        return {"value": cb["value"], "unit": "Mcells/s", "cores": cb["cores"], "kind": "port",
+                "sample": f"the first {cb['clouds']} clouds ({cb['cells']} cells), each its own diagram, on "
+                          f"{cb['cores']} threads"}
+    except Exception as exc:
+        return {"value": None, "unit": "Mcells/s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
+
+
 def run_gpu(args, spec, rank, world, local):
     import torch
 
     import paragram_b200 as pg
     import paragram_b200.cuda as pc
-    from paragram_b200 import dist
+    from paragram_b200 import dist, learned
 
     dev = torch.device(f"cuda:{local}")
     torch.cuda.set_device(dev)
+    if spec["kind"] == "surfaces":
+        return run_batch_gpu(args, spec, rank, world, local, dev)
     pts, w = make_points(spec, seed=rank)
     n = pts.shape[0]
     h_pts = torch.from_numpy(pts).pin_memory()
     h_w = torch.from_numpy(w).pin_memory() if w is not None else None
     d_pts = h_pts.to(dev)
-    d_w = h_w.to(dev) if h_w is not None else None
+    d_w = h_w.to(dev)[:, None] if h_w is not None else None
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    use_model = args.workload in LEARNED and not args.plain
+    model = train_info = None
+    if use_model:
+        model, train_info = train_model(dev, rank)
+    blob = model.blob if model is not None else None
 
-    def step_device():
-        if d_w is None:
-            return pc._run(d_pts, None, 8, False, None, None, -1, profile=True)
-        return pc._run(d_pts, d_w[:, None], 8, False, None, None, -1, profile=True)
+    def step_device(with_model=True):
+        return pc._run(d_pts, d_w, 8, False, None, None, -1, profile=True,
+                       model=blob if with_model else None)
 
     def step_e2e():
         x = h_pts.to(dev, non_blocking=True)
         if h_w is None:
-            d = pg.voronoi_diagram(x)
+            d = learned.voronoi_diagram(x, model) if model is not None else pg.voronoi_diagram(x)
         else:
             d = pg.power_diagram(x, h_w.to(dev, non_blocking=True))
-        a = d.adjacency.to("cpu", non_blocking=False)
-        o = d.offsets.to("cpu")
-        s = d.status.to("cpu")
-        return a, o, s
+        return d.adjacency.to("cpu"), d.offsets.to("cpu"), d.status.to("cpu")
 
     for _ in range(args.warmup):
         step_device()
+        if use_model:
+            step_device(False)
     torch.cuda.synchronize(dev)
     dist.barrier()
-
-    times, cell_ms, launches = [], [], 0
     with ClockSampler(local) as clocks:
-        for _ in range(args.steps):
-            flush.fill_(1.0)
-            torch.cuda.synchronize(dev)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            adj, off, st = step_device()
-            e1.record()
-            torch.cuda.synchronize(dev)
-            times.append(e0.elapsed_time(e1))
-            prof = pc.last_profile()
-            cell_ms.append(prof["cells_ms"])
-            launches += int(prof["launches"])
+        times, cell_ms, launches, (adj, off, st) = _timed(step_device, args.steps, dev, flush)
+        plain = _timed(lambda: step_device(False), args.steps, dev, flush) if use_model else None
     dist.barrier()
     torch.cuda.synchronize(dev)
     total_ms = dist.reduce_max(sum(times), dev)
     total_cells = dist.reduce_sum(float(n) * args.steps, dev)
     value = total_cells / (total_ms / 1e3) / 1e6
+    plain_value = None
+    if plain is not None:
+        plain_value = total_cells / (dist.reduce_max(sum(plain[0]), dev) / 1e3) / 1e6
 
     # end-to-end through the public API from pinned host memory
     for _ in range(max(1, args.warmup // 2)):
         step_e2e()
     torch.cuda.synchronize(dev)
     dist.barrier()
-    e2e_times, d2h = [], 0
-    for _ in range(args.steps):
-        flush.fill_(1.0)
-        torch.cuda.synchronize(dev)
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        a, o, s = step_e2e()
-        e1.record()
-        torch.cuda.synchronize(dev)
-        e2e_times.append(e0.elapsed_time(e1))
-        d2h = a.numel() * 4 + o.numel() * 4 + s.numel() * 4
+    e2e_times, _, _, (a, o, s) = _timed(step_e2e, args.steps, dev, flush)
+    d2h = a.numel() * 4 + o.numel() * 4 + s.numel() * 4
     e2e_ms = dist.reduce_max(sum(e2e_times), dev)
     e2e_value = total_cells / (e2e_ms / 1e3) / 1e6
     h2d = n * 12 + (n * 4 if h_w is not None else 0)
+    # counters of one more (untimed) build: escalations, fallback rate
+    _, cnt = pc.build_with_stats(d_pts, d_w, model=blob)
 
     if rank == 0:
         off_np = off.cpu().numpy()
         flops, nbytes = algorithmic_work(off_np, spec["weighted"])
         cell_s = statistics.mean(cell_ms) / 1e3
         csum = clocks.summary()
-        peaks = {}
-        try:
-            peaks = json.load(open(MEASURED_PEAKS))
-        except (OSError, ValueError):
-            pass
-        peak = fp32_peak_tflops(peaks.get("sm_max_mhz") or csum.get("sm_max_mhz"))
-        achieved = flops / cell_s / 1e12 if cell_s > 0 else None
-        traffic = read_traffic_per_launch()
-        hbm_peak = peaks.get("hbm_gbs", 6650.0)
-        cpu = None
-        if world == 1 and not args.no_cpu_baseline:
-            try:
-                cb = cpu_oracle_rate(pts, w, args.cpu_sample)
-                cpu = {"value": cb["value"], "unit": "Mcells/s", "cores": cb["cores"], "kind": "port",
-                       "sample": f"{cb['cells']} of {n} cells; kd-tree {cb['tree_s']:.2f} s + cells "
-                                 f"{cb['cells_s']:.2f} s on {cb['cores']} threads, extrapolated to all cells"}
-            except Exception as exc:  # the baseline must not hide the GPU number
-                cpu = {"value": None, "unit": "Mcells/s", "cores": 0, "kind": "port", "sample": f"failed: {exc}"}
+        config = {"workload": args.workload, "n_points": n, "weighted": spec["weighted"],
+                  "l2": "flushed between steps (256 MiB write)",
+                  "parallelism": f"independent diagram per GPU x{world}",
+                  "predicates": "FP32 filtered, FP64 / exact escalation",
+                  "escalation": {"fp32_tests_per_cell": cnt["tests"] / n,
+                                 "fp64_fraction": cnt["fp64_escalations"] / max(cnt["tests"], 1),
+                                 "exact_fraction": cnt["exact_escalations"] / max(cnt["tests"], 1),
+                                 "fp64_vertices_per_cell": cnt["vertex64"] / n}}
+        if use_model:
+            config["search_radius"] = "learned (MLP 16-64-64-2, BF16, trained before timing)"
+            config["learned"] = dict(train_info, fallback_rate=cnt["hint_misses"] / n,
+                                     capped_cells=(cnt["hint_hits"] + cnt["hint_misses"]) / n)
+            config["plain"] = {"value": plain_value, "unit": "Mcells/s", "ms_per_step": statistics.mean(plain[0]),
+                               "cell_pass_ms": statistics.mean(plain[1])}
+            config["learned_over_plain"] = value / plain_value if plain_value else None
         line = {
             "metric": "Mcells/s",
             "value": value,
@@ -317,21 +422,78 @@ def run_gpu(args, spec, rank, world, local):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": args.workload, "n_points": n, "weighted": spec["weighted"],
-                       "l2": "flushed between steps (256 MiB write)",
-                       "parallelism": f"independent diagram per GPU x{world}",
-                       "predicates": "FP32 filtered, FP64 / exact escalation"},
+            "config": config,
             "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "kernel": "k_cells_fast (cell pass)", "cell_pass_ms": cell_s * 1e3,
-                         "algorithmic_flops": flops, "algorithmic_bytes": nbytes,
-                         "hbm_frac": (nbytes / cell_s / 1e9) / hbm_peak if cell_s > 0 else None,
-                         "peak_note": "nominal FP32 FMA peak 148 SM x 128 lanes x 2 x max SM clock "
-                                      "(MEASURED_PEAKS has no FP32 figure)"},
-            "cpu_baseline": cpu,
+            "roofline": _roofline(flops, nbytes, cell_s, csum, "k_cells_fast (cell pass)",
+                                  read_traffic_per_launch() if args.workload == "clustered_voronoi_5m" else None),
+            "cpu_baseline": _cpu_baseline(args, world, pts, w, n),
             "clocks": csum,
             "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_batch_gpu(args, spec, rank, world, local, dev):
+    """256 surface clouds of uneven size in one build (CUDA graph replay), per-cloud Diagrams."""
+    import torch
+
+    import paragram_b200.cuda as pc
+    from paragram_b200 import dist
+    from paragram_b200.batch import build_batch
+
+    clouds, _ = make_points(spec, seed=rank)
+    n = int(sum(len(c) for c in clouds))
+    h_clouds = [torch.from_numpy(c).pin_memory() for c in clouds]
+    d_clouds = [c.to(dev) for c in h_clouds]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    build_batch(d_clouds, graph=False)
+    launches_per_build = int(pc.last_profile()["launches"]) + 1  # + adjacency emission
+
+    def step():
+        return build_batch(d_clouds, graph=True)
+
+    def step_e2e():
+        ds = build_batch([c.to(dev, non_blocking=True) for c in h_clouds], graph=True)
+        return [(d.adjacency.to("cpu"), d.offsets.to("cpu"), d.status.to("cpu")) for d in ds]
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    with ClockSampler(local) as clocks:
+        times, _, _, ds = _timed(step, args.steps, dev, flush)
+    dist.barrier()
+    total_ms = dist.reduce_max(sum(times), dev)
+    total_cells = dist.reduce_sum(float(n) * args.steps, dev)
+    value = total_cells / (total_ms / 1e3) / 1e6
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    e2e_times, _, _, res = _timed(step_e2e, args.steps, dev, flush)
+    e2e_value = total_cells / (dist.reduce_max(sum(e2e_times), dev) / 1e3) / 1e6
+    d2h = sum(a.numel() * 4 + o.numel() * 4 + s.numel() * 4 for a, o, s in res)
+    if rank == 0:
+        flops = nbytes = 0.0
+        status = np.zeros(6, np.int64)
+        for d in ds:
+            f, b = algorithmic_work(d.offsets.cpu().numpy(), False)
+            flops += f
+            nbytes += b
+            status += np.bincount(d.status.cpu().numpy(), minlength=6)[:6]
+        csum = clocks.summary()
+        step_s = statistics.mean(times) / 1e3
+        line = {
+            "metric": "Mcells/s", "value": value, "unit": "Mcells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": statistics.mean(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": args.workload, "clouds": len(clouds), "n_points": n,
+                       "cloud_sizes": [int(min(len(c) for c in clouds)), int(max(len(c) for c in clouds))],
+                       "l2": "flushed between steps (256 MiB write)", "launch": "one CUDA graph per batch shape",
+                       "status_counts": status.tolist(), "parallelism": f"independent batch per GPU x{world}"},
+            "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": n * 12, "d2h_bytes_per_step": d2h},
+            "roofline": _roofline(flops, nbytes, step_s, csum, "whole batched build (graph replay)", None),
+            "cpu_baseline": _cpu_baseline_clouds(args, world, clouds),
+            "clocks": csum,
+            "gpu_launches": launches_per_build * args.steps,
         }
         print(json.dumps(line), flush=True)
 
@@ -345,6 +507,7 @@ def main():
     ap.add_argument("--workload", default="clustered_voronoi_5m", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--plain", action="store_true", help="time the plain build only (no learned radius)")
     args = ap.parse_args()
     spec = WORKLOADS[args.workload]
     from paragram_b200 import dist
