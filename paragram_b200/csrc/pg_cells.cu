@@ -35,6 +35,7 @@
 // reference MAX_VERTS) and plane_overflow (1) only if even 256 slots overflow.
 #include <cfloat>
 #include <climits>
+#include <type_traits>
 
 #include "pg_common.cuh"
 #include "pg_exact.cuh"
@@ -51,6 +52,14 @@ constexpr float kEps = 5.9604645e-8f; // 2^-24
 constexpr float kVertex64Rel = PG_VERTEX64_REL;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
+// A vertex is the triangle of its three plane slots, packed in 10-bit fields;
+// a boundary edge (x, y) packs its two plane slots in 16-bit fields.
+__host__ __device__ __forceinline__ unsigned tri_pack(unsigned a, unsigned b, unsigned c)
+{
+    return a | (b << 10) | (c << 20);
+}
+__host__ __device__ __forceinline__ unsigned tri_get(unsigned t, int e) { return (t >> (10 * e)) & 1023u; }
+
 template <int CAP, int STACK> struct CellMem
 {
     float4 pl[CAP];   // plane (n.x, n.y, n.z, h): interior n.x <= h (relative to the seed)
@@ -58,8 +67,8 @@ template <int CAP, int STACK> struct CellMem
     float pe[CAP];    // bound on |h - h_exact|
     float vr[CAP];    // (|X| + psi)^2, upper bound on |X_exact|^2
     int pid[CAP];     // >= 0: sorted point index; < 0: -1 - box code
-    unsigned vt[CAP]; // plane slots p0 | p1 << 8 | p2 << 16 (oriented)
-    unsigned eb[CAP]; // boundary edges x | y << 8 of the clip in progress, by rank
+    unsigned vt[CAP]; // plane slots of the vertex, tri_pack(p0, p1, p2) (oriented)
+    unsigned eb[CAP]; // boundary edges x | y << 16 of the clip in progress, by rank
     int stk[STACK];   // pending BVH references (unordered)
     float skey[STACK]; // lower bound of the bisector distance of any point of the pending node
     unsigned long long cnt[kNumStats]; // per-warp statistics (written by lane 0)
@@ -91,6 +100,7 @@ struct CellArgs
     int big_pass;
     int64_t big_cap;
     char *slabs;
+    char *huge_slabs;
     int inline_big; // rebuild deferred cells right away in the same kernel (warp path)
     float *radius_out; // optional per-cell diagnostics (original ids)
     int4 *work_out;
@@ -355,10 +365,10 @@ __device__ __forceinline__ void cell_init(CellMem<CAP, STACK> &m, WarpState<CAP>
         float vr;
         m.vx[lane] = make_vertex(m.pl[p0], m.pe[p0], m.pl[p1], m.pe[p1], m.pl[p2], m.pe[p2], vr);
         m.vr[lane] = vr;
-        m.vt[lane] = (unsigned)p0 | ((unsigned)p1 << 8) | ((unsigned)p2 << 16);
+        m.vt[lane] = tri_pack((unsigned)p0, (unsigned)p1, (unsigned)p2);
     }
     __syncwarp();
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < WarpState<CAP>::W; ++k)
         ws.valid[k] = k == 0 ? 0xFFu : 0u;
     ws.np = 6;
@@ -370,7 +380,7 @@ __device__ __forceinline__ void cell_init(CellMem<CAP, STACK> &m, WarpState<CAP>
 template <int W> __device__ __forceinline__ int count_bits(const unsigned (&m)[W])
 {
     int c = 0;
-#pragma unroll
+#pragma unroll(W > 8 ? 1 : W)
     for (int k = 0; k < W; ++k)
         c += __popc(m[k]);
     return c;
@@ -381,29 +391,29 @@ template <int CAP, int STACK> __device__ __forceinline__ void gc_planes(CellMem<
 {
     constexpr int W = CAP / 32;
     unsigned lm[W];
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         lm[k] = 0;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         if ((ws.valid[k] >> lane) & 1u)
         {
             unsigned t = m.vt[k * 32 + lane];
-            unsigned p[3] = {t & 255u, (t >> 8) & 255u, (t >> 16) & 255u};
+            unsigned p[3] = {tri_get(t, 0), tri_get(t, 1), tri_get(t, 2)};
 #pragma unroll
             for (int e = 0; e < 3; ++e)
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
                 for (int kk = 0; kk < W; ++kk)
                     if ((int)(p[e] >> 5) == kk)
                         lm[kk] |= 1u << (p[e] & 31u);
         }
     unsigned live[W];
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         live[k] = __reduce_or_sync(kFull, lm[k]);
     int pre[W];
     int acc = 0;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
         pre[k] = acc;
@@ -412,7 +422,7 @@ template <int CAP, int STACK> __device__ __forceinline__ void gc_planes(CellMem<
     float4 tpl[W];
     float tpe[W];
     int tpid[W];
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
         int p = k * 32 + lane;
@@ -424,7 +434,7 @@ template <int CAP, int STACK> __device__ __forceinline__ void gc_planes(CellMem<
         }
     }
     __syncwarp();
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
         int p = k * 32 + lane;
@@ -436,7 +446,7 @@ template <int CAP, int STACK> __device__ __forceinline__ void gc_planes(CellMem<
             m.pid[q] = tpid[k];
         }
     }
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         if ((ws.valid[k] >> lane) & 1u)
         {
@@ -445,13 +455,13 @@ template <int CAP, int STACK> __device__ __forceinline__ void gc_planes(CellMem<
 #pragma unroll
             for (int e = 0; e < 3; ++e)
             {
-                unsigned p = (t >> (8 * e)) & 255u;
+                unsigned p = tri_get(t, e);
                 unsigned q = 0;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
                 for (int kk = 0; kk < W; ++kk)
                     if ((int)(p >> 5) == kk)
                         q = pre[kk] + __popc(live[kk] & ((1u << (p & 31u)) - 1u));
-                out |= q << (8 * e);
+                out |= q << (10 * e);
             }
             m.vt[k * 32 + lane] = out;
         }
@@ -479,7 +489,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
     constexpr int W = CAP / 32;
     unsigned rem[W];
     unsigned tri[W];
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
         int r = 0;
@@ -493,7 +503,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
             {
                 unsigned t = m.vt[slot];
                 int used = 0;
-                r = side_exact(m.pid[t & 255u], m.pid[(t >> 8) & 255u], m.pid[(t >> 16) & 255u], q.id, A.pts, A.oid,
+                r = side_exact(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], q.id, A.pts, A.oid,
                                ws.box, ws.s, ws.soid, &used);
                 atomicAdd(&m.cnt[kStatFp64], 1ull);
                 if (used)
@@ -511,7 +521,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
     }
     PG_COUNT(m, lane, kStatTests, count_bits(ws.valid));
     bool any = false, all = true;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
         any = any || rem[k] != 0u;
@@ -522,7 +532,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
     if (all)
     {
         ws.flags |= kFlagEmpty;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
         for (int k = 0; k < W; ++k)
             ws.valid[k] = 0;
         return kClipEmptied;
@@ -533,7 +543,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         if (ws.np >= CAP)
             return kClipDefer;
         // plane slots were renumbered: reload the removed triangles
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
         for (int k = 0; k < W; ++k)
             if ((rem[k] >> lane) & 1u)
                 tri[k] = m.vt[k * 32 + lane];
@@ -546,12 +556,13 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         m.pid[P] = q.id;
     }
     // boundary edges of the removed region
-    unsigned bf = 0; // bit k*3+e: edge e of my removed vertex in word k is a boundary edge
-#pragma unroll
+    using Bits = typename std::conditional<(3 * W > 32), unsigned long long, unsigned>::type;
+    Bits bf = 0; // bit k*3+e: edge e of my removed vertex in word k is a boundary edge
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         if ((rem[k] >> lane) & 1u)
-            bf |= 7u << (3 * k);
-#pragma unroll
+            bf |= (Bits)7u << (3 * k);
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
         unsigned mm = rem[k];
@@ -560,12 +571,12 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
             int b = __ffs(mm) - 1;
             mm &= mm - 1;
             unsigned t = __shfl_sync(kFull, tri[k], b);
-            unsigned t0 = t & 255u, t1 = (t >> 8) & 255u, t2 = (t >> 16) & 255u;
-#pragma unroll
+            unsigned t0 = tri_get(t, 0), t1 = tri_get(t, 1), t2 = tri_get(t, 2);
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
             for (int kk = 0; kk < W; ++kk)
             {
                 unsigned my = tri[kk];
-                unsigned m0 = my & 255u, m1 = (my >> 8) & 255u, m2 = (my >> 16) & 255u;
+                unsigned m0 = tri_get(my, 0), m1 = tri_get(my, 1), m2 = tri_get(my, 2);
                 unsigned xs[3] = {m0, m1, m2}, ys[3] = {m1, m2, m0};
 #pragma unroll
                 for (int e = 0; e < 3; ++e)
@@ -573,7 +584,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
                     unsigned x = xs[e], y = ys[e];
                     bool rev = (t0 == y && t1 == x) || (t1 == y && t2 == x) || (t2 == y && t0 == x);
                     if (rev)
-                        bf &= ~(1u << (3 * kk + e));
+                        bf &= ~((Bits)1u << (3 * kk + e));
                 }
             }
         }
@@ -581,16 +592,16 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
     // list the boundary edges by rank in the warp's edge buffer
     const unsigned lt = (1u << lane) - 1u;
     int nb = 0;
-#pragma unroll
+#pragma unroll(W > 8 ? 1 : 3 * W)
     for (int f = 0; f < 3 * W; ++f)
     {
         unsigned bal = __ballot_sync(kFull, (bf >> f) & 1u);
         if ((bf >> f) & 1u)
         {
             unsigned my = tri[f / 3];
-            unsigned x = (my >> (8 * (f % 3))) & 255u;
-            unsigned y = (my >> (8 * ((f % 3 + 1) % 3))) & 255u;
-            m.eb[nb + __popc(bal & lt)] = x | (y << 8);
+            unsigned x = tri_get(my, f % 3);
+            unsigned y = tri_get(my, (f % 3 + 1) % 3);
+            m.eb[nb + __popc(bal & lt)] = x | (y << 16);
         }
         nb += __popc(bal);
     }
@@ -598,14 +609,14 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
     if (nv_new > CAP)
         return kClipDefer;
     unsigned fr[W];
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         fr[k] = ~ws.valid[k] | rem[k];
     __syncwarp(); // edge list, plane P and all reads of removed triangles are done
     float4 pP = m.pl[P];
     float eP = m.pe[P];
     unsigned nbits[W];
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         nbits[k] = 0;
     // lane r builds the vertex (P, x, y) of the r-th boundary edge in the r-th free slot
@@ -615,9 +626,9 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         if (r < nb)
         {
             unsigned xy = m.eb[r];
-            unsigned x = xy & 255u, y = xy >> 8;
+            unsigned x = xy & 0xFFFFu, y = xy >> 16;
             int rr = r, slot = -1;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
             for (int k = 0; k < W; ++k)
             {
                 int c = __popc(fr[k]);
@@ -632,8 +643,8 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
                 float4 X = make_vertex(pP, eP, m.pl[x], m.pe[x], m.pl[y], m.pe[y], vr);
                 m.vx[slot] = X;
                 m.vr[slot] = vr;
-                m.vt[slot] = (unsigned)P | (x << 8) | (y << 16);
-#pragma unroll
+                m.vt[slot] = tri_pack((unsigned)P, x, y);
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
                 for (int k = 0; k < W; ++k)
                     if ((slot >> 5) == k)
                         nbits[k] |= 1u << (slot & 31);
@@ -643,7 +654,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         }
     }
     // ill-conditioned in FP32: rebuild in FP64 so that the empty sphere stays tight
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
         unsigned mm = nbits[k];
@@ -656,14 +667,14 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
             {
                 unsigned t = m.vt[slot];
                 float vr = m.vr[slot];
-                m.vx[slot] = make_vertex64(m.pid[t & 255u], m.pid[(t >> 8) & 255u], m.pid[(t >> 16) & 255u], A.pts, A.oid,
+                m.vx[slot] = make_vertex64(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], A.pts, A.oid,
                                            ws.box, ws.s, X, vr, vr);
                 m.vr[slot] = vr;
                 atomicAdd(&m.cnt[kStatVertex64], 1ull);
             }
         }
     }
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         ws.valid[k] = (ws.valid[k] & ~rem[k]) | __reduce_or_sync(kFull, nbits[k]);
     __syncwarp();
@@ -674,7 +685,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
 template <int CAP, int STACK> __device__ __forceinline__ void update_rsafe(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int lane)
 {
     float mx = 0.0f;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < CAP / 32; ++k)
         if ((ws.valid[k] >> lane) & 1u)
             mx = fmaxf(mx, m.vr[k * 32 + lane]);
@@ -699,7 +710,7 @@ __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP>
         // FP32 pre-check restricted to the vertices whose empty sphere reaches the
         // leaf's box: a point of the leaf can remove no other vertex.
         bool may = false;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
         for (int k = 0; k < CAP / 32; ++k)
         {
             unsigned mm = vmask.w[k] & ws.valid[k];
@@ -777,7 +788,7 @@ __device__ __forceinline__ bool node_vertex_mask(const CellMem<CAP, STACK> &m, c
     float dm = mw - ws.s.w;
     float dmu = dm > 0.0f ? dm * (1.0f + 1e-6f) : dm * (1.0f - 1e-6f);
     bool any = false;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < CAP / 32; ++k)
     {
         bool may = false;
@@ -817,10 +828,10 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
         return true;
     }
     unsigned lm[W];
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         lm[k] = 0;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         if ((ws.valid[k] >> lane) & 1u)
         {
@@ -828,8 +839,8 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
 #pragma unroll
             for (int e = 0; e < 3; ++e)
             {
-                unsigned p = (t >> (8 * e)) & 255u;
-#pragma unroll
+                unsigned p = tri_get(t, e);
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
                 for (int kk = 0; kk < W; ++kk)
                     if ((int)(p >> 5) == kk)
                         lm[kk] |= 1u << (p & 31u);
@@ -838,7 +849,7 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
     int o[W];
     unsigned has[W];
     int cnt = 0;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
         unsigned live = __reduce_or_sync(kFull, lm[k]);
@@ -854,10 +865,10 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
         cnt += __popc(has[k]);
     }
     int rnk[W];
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         rnk[k] = 0;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
         unsigned mm = has[k];
@@ -866,7 +877,7 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
             int b = __ffs(mm) - 1;
             mm &= mm - 1;
             int v = __shfl_sync(kFull, o[k], b);
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
             for (int kk = 0; kk < W; ++kk)
                 rnk[kk] += (v < o[kk]);
         }
@@ -877,6 +888,11 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
     int st = nverts > kMaxVertsRef ? kVertexOverflow : kSuccess;
     if (ws.flags & kFlagDefer)
         st = kPlaneOverflow; // only reachable in the large-capacity pass
+    if (big && cnt > kBigRowWidth)
+    {
+        st = kPlaneOverflow; // more faces than a deferred row holds: keep the first ones
+        cnt = kBigRowWidth;
+    }
     int *row;
     if (big)
     {
@@ -894,9 +910,9 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
         if (lane == 0)
             A.deg[oi] = cnt;
     }
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
-        if (o[k] != INT_MAX)
+        if (o[k] != INT_MAX && rnk[k] < cnt)
             row[rnk[k]] = o[k];
     if (lane == 0)
         A.status[oi] = st;
@@ -1137,7 +1153,7 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
     if (ref_is_leaf(ws.root))
     {
         VMask<CAP / 32> allv;
-#pragma unroll
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
         for (int k = 0; k < CAP / 32; ++k)
             allv.w[k] = 0xFFFFFFFFu;
         leaf_batch<CAP, STACK, GUESS>(m, ws, ws.root, i, A, lane, allv);
@@ -1190,10 +1206,40 @@ template <int CAP, int STACK> __device__ void flush_stats(CellMem<CAP, STACK> &m
         atomicAdd(&A.stats[lane], m.cnt[lane]);
 }
 
+// Rebuild cell i with 512 vertex / plane slots and a 2048-entry queue: the
+// rare cell that outgrew the 256 slots (long cells of surface data reach a
+// few hundred vertices). Its state lives in one of kHugeSlabs global slabs,
+// one per such cell and build; returns false when they are used up (the
+// caller keeps its plane-overflow result).
+__device__ __noinline__ bool huge_cell(const CellArgs &A, int i, int lane, int slot)
+{
+    int hs = 0;
+    if (lane == 0)
+        hs = atomicAdd(&A.counters[4], 1);
+    hs = __shfl_sync(kFull, hs, 0);
+    if (hs >= kHugeSlabs)
+        return false;
+    auto &m = *reinterpret_cast<CellMem<kCapHuge, kStackHuge> *>(A.huge_slabs +
+                                                                  hs * sizeof(CellMem<kCapHuge, kStackHuge>));
+    WarpState<kCapHuge> ws;
+    if (lane < kNumStats)
+        m.cnt[lane] = 0;
+    __syncwarp();
+    process_cell<kCapHuge, kStackHuge, false, false>(m, ws, i, A, lane);
+    write_diagnostics(m, ws, A, lane);
+    if ((ws.flags & kFlagError) && lane == 0)
+        atomicExch(&A.counters[2], 1);
+    ws.si = slot;
+    write_outputs(m, ws, A, lane, true);
+    flush_stats(m, A, lane);
+    return true;
+}
+
 // Rebuild cell i with 256 vertex / plane slots and a 1024-entry queue in this
 // warp's global slab. Called by the warp whose shared-memory cell outgrew its
 // 64 slots, right away, so that the few expensive cells overlap with the rest
-// of the cell pass instead of forming a tail after it.
+// of the cell pass instead of forming a tail after it. A cell that outgrows the
+// 256 slots too is rebuilt once more by huge_cell.
 template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, int i, int lane)
 {
     size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1210,6 +1256,11 @@ template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, i
     write_diagnostics(m, ws, A, lane);
     if ((ws.flags & kFlagError) && lane == 0)
         atomicExch(&A.counters[2], 1);
+    if ((ws.flags & kFlagDefer) && slot < A.big_cap && huge_cell(A, i, lane, slot))
+    {
+        flush_stats(m, A, lane);
+        return;
+    }
     if (slot < A.big_cap)
     {
         ws.si = slot; // deferred-row slot
@@ -1805,6 +1856,7 @@ int tcell_threads() { return 148 * 1024; }
 size_t tcell_slab_bytes() { return sizeof(TSlab) * (size_t)(tcell_threads() / 32); }
 
 int big_warps() { return 148 * 4 * kWarpsPerBlock; } // one slab per resident warp (<= 4 blocks / SM)
+size_t huge_slab_bytes() { return sizeof(CellMem<kCapHuge, kStackHuge>) * (size_t)kHugeSlabs; }
 size_t big_slab_bytes() { return sizeof(CellMem<kCapBig, kStackBig>) * (size_t)big_warps(); }
 
 static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
@@ -1834,6 +1886,7 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.big_pass = 0;
     A.big_cap = 0;
     A.slabs = (char *)ws.big_slabs;
+    A.huge_slabs = (char *)ws.huge_slabs;
     A.inline_big = 0;
     A.radius_out = cl.radius_out;
     A.work_out = reinterpret_cast<int4 *>(cl.work_out);

@@ -25,6 +25,9 @@ constexpr int kCapFast = 64;        // vertex / plane slots of a cell in shared 
 constexpr int kStackFast = 256;     // pending BVH nodes of a cell in shared memory
 constexpr int kCapBig = 256;        // vertex / plane slots of a deferred cell (global memory)
 constexpr int kStackBig = 1024;     // traversal stack of a deferred cell
+constexpr int kCapHuge = 512;       // vertex / plane slots of a cell that outgrew kCapBig (rare)
+constexpr int kStackHuge = 2048;
+constexpr int kHugeSlabs = 256;     // such cells per build (global-memory state each)
 constexpr int kRowWidth = 36;       // row slots per cell: a cell with <= 64 vertices has <= 34 faces
 constexpr int kBigRowWidth = kCapBig; // row slots of a deferred cell
 constexpr int kWarpsPerBlock = 8;   // cell kernel block = 8 warps, one cell per warp at a time
@@ -130,6 +133,7 @@ struct Workspace
     int *big_list;        // [N] sorted slots deferred to the large-capacity pass
     int *big_rows;        // [big_cap * kBigRowWidth]
     void *big_slabs;      // per-warp state of the large-capacity pass
+    void *huge_slabs;     // [kHugeSlabs] state of cells that outgrew the large capacity
     void *tslabs;         // per-warp state of the thread-per-cell pass
     // CSR
     int *cnt;             // [N] kept directed entries per row
@@ -141,6 +145,7 @@ struct Workspace
 
 int big_warps();   // number of warps of the large-capacity pass
 size_t big_slab_bytes();
+size_t huge_slab_bytes();
 int tcell_threads(); // resident threads of the thread-per-cell pass
 size_t tcell_slab_bytes();
 size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws);

@@ -50,3 +50,20 @@ def test_batch_power(dev, oracle):
         got = _np(d)
         exp = oracle.diagram(p, w)
         assert all(np.array_equal(a, b) for a, b in zip(got, exp))
+
+
+def test_cells_beyond_256_vertices(dev, oracle):
+    """Surface clouds have rare long cells that outgrow 256 vertex slots (the 512-slot tier):
+    cloud 191 has a final cell of 292 vertices, cloud 56 one that exceeds 256 slots only while
+    it is being clipped. Status vertex_overflow and complete sorted rows, as the oracle."""
+    import paragram_b200 as pg
+    from paragram_b200 import workloads as W
+
+    clouds = W.surface_clouds(num_clouds=256, seed=0)
+    for k, final_over in ((191, True), (56, False)):
+        c = clouds[k]
+        got = _np(pg.voronoi_diagram(torch.from_numpy(c).to(dev)))
+        exp = oracle.diagram(c)
+        assert all(np.array_equal(a, b) for a, b in zip(got, exp)), k
+        assert (got[2] == 1).sum() == 0
+        assert (oracle.cells(c).nverts.max() > 256) == final_over
