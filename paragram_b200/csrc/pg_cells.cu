@@ -45,6 +45,14 @@ namespace pg
 {
 
 constexpr float kEps = 5.9604645e-8f; // 2^-24
+// resident blocks per SM of the two register budgets of the cell kernel (blocks_per_sm 2 and 3)
+#ifndef PG_MINB_LO
+#define PG_MINB_LO 2
+#endif
+#ifndef PG_MINB_HI
+#define PG_MINB_HI 3
+#endif
+constexpr int kMinBlocksLo = PG_MINB_LO, kMinBlocksHi = PG_MINB_HI;
 // A vertex whose FP32 error radius exceeds this fraction of its L1 norm is rebuilt in FP64.
 #ifndef PG_VERTEX64_REL
 #define PG_VERTEX64_REL 3e-4f
@@ -73,7 +81,16 @@ template <int CAP, int STACK> struct CellMem
     float skey[STACK]; // lower bound of the bisector distance of any point of the pending node
     unsigned long long cnt[kNumStats]; // per-warp statistics (written by lane 0)
     unsigned long long cnt0[3];        // nodes, leaves, candidates at the start of the current cell
+    unsigned et[CAP * CAP / 32];       // edge table of the clip in progress (all zero between clips)
 };
+
+// Clear a warp's edge table (once, before its first clip).
+template <int CAP, int STACK> __device__ __forceinline__ void clear_edges(CellMem<CAP, STACK> &m, int lane)
+{
+    for (int k = lane; k < CAP * CAP / 32; k += 32)
+        m.et[k] = 0u;
+    __syncwarp();
+}
 
 struct CellArgs
 {
@@ -555,40 +572,49 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         m.pe[P] = q.eh;
         m.pid[P] = q.id;
     }
-    // boundary edges of the removed region
+    // boundary edges of the removed region: the directed edge x->y of a removed
+    // triangle is a boundary edge iff y->x is not an edge of another removed
+    // triangle. The removed triangles mark their edges in the warp's edge table
+    // (bit x * CAP + y), each lane tests the reverses of its own edges, then the
+    // marks are cleared (the table is all zero between clips).
     using Bits = typename std::conditional<(3 * W > 32), unsigned long long, unsigned>::type;
     Bits bf = 0; // bit k*3+e: edge e of my removed vertex in word k is a boundary edge
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         if ((rem[k] >> lane) & 1u)
-            bf |= (Bits)7u << (3 * k);
-#pragma unroll(CAP > 256 ? 1 : CAP / 32)
-    for (int k = 0; k < W; ++k)
-    {
-        unsigned mm = rem[k];
-        while (mm)
         {
-            int b = __ffs(mm) - 1;
-            mm &= mm - 1;
-            unsigned t = __shfl_sync(kFull, tri[k], b);
-            unsigned t0 = tri_get(t, 0), t1 = tri_get(t, 1), t2 = tri_get(t, 2);
-#pragma unroll(CAP > 256 ? 1 : CAP / 32)
-            for (int kk = 0; kk < W; ++kk)
-            {
-                unsigned my = tri[kk];
-                unsigned m0 = tri_get(my, 0), m1 = tri_get(my, 1), m2 = tri_get(my, 2);
-                unsigned xs[3] = {m0, m1, m2}, ys[3] = {m1, m2, m0};
+            unsigned t = tri[k];
 #pragma unroll
-                for (int e = 0; e < 3; ++e)
-                {
-                    unsigned x = xs[e], y = ys[e];
-                    bool rev = (t0 == y && t1 == x) || (t1 == y && t2 == x) || (t2 == y && t0 == x);
-                    if (rev)
-                        bf &= ~((Bits)1u << (3 * kk + e));
-                }
+            for (int e = 0; e < 3; ++e)
+            {
+                unsigned bit = tri_get(t, e) * CAP + tri_get(t, (e + 1) % 3);
+                atomicOr(&m.et[bit >> 5], 1u << (bit & 31u));
             }
         }
-    }
+    __syncwarp();
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+        if ((rem[k] >> lane) & 1u)
+        {
+            unsigned t = tri[k];
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+            {
+                unsigned rbit = tri_get(t, (e + 1) % 3) * CAP + tri_get(t, e);
+                if (!((m.et[rbit >> 5] >> (rbit & 31u)) & 1u))
+                    bf |= (Bits)1u << (3 * k + e);
+            }
+        }
+    __syncwarp();
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+        if ((rem[k] >> lane) & 1u)
+        {
+            unsigned t = tri[k];
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+                m.et[(tri_get(t, e) * CAP + tri_get(t, (e + 1) % 3)) >> 5] = 0u;
+        }
     // list the boundary edges by rank in the warp's edge buffer
     const unsigned lt = (1u << lane) - 1u;
     int nb = 0;
@@ -1224,7 +1250,7 @@ __device__ __noinline__ bool huge_cell(const CellArgs &A, int i, int lane, int s
     WarpState<kCapHuge> ws;
     if (lane < kNumStats)
         m.cnt[lane] = 0;
-    __syncwarp();
+    clear_edges(m, lane);
     process_cell<kCapHuge, kStackHuge, false, false>(m, ws, i, A, lane);
     write_diagnostics(m, ws, A, lane);
     if ((ws.flags & kFlagError) && lane == 0)
@@ -1251,7 +1277,7 @@ template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, i
     if (lane == 0)
         slot = atomicAdd(&A.counters[1], 1);
     slot = __shfl_sync(kFull, slot, 0);
-    __syncwarp();
+    clear_edges(m, lane);
     process_cell<kCapBig, kStackBig, GUESS, false>(m, ws, i, A, lane);
     write_diagnostics(m, ws, A, lane);
     if ((ws.flags & kFlagError) && lane == 0)
@@ -1281,7 +1307,7 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
     WarpState<CAP> ws;
     if (lane < kNumStats)
         m.cnt[lane] = 0;
-    __syncwarp();
+    clear_edges(m, lane);
     int64_t count = A.big_pass ? min((int64_t)A.counters[1], A.big_cap) : (A.end - A.begin);
     int *ctr = A.big_pass ? &A.counters[3] : &A.counters[0];
     for (;;)
@@ -1855,7 +1881,7 @@ __global__ void __launch_bounds__(256, 4) k_tcells(CellArgs A, TSlab *slabs)
 int tcell_threads() { return 148 * 1024; }
 size_t tcell_slab_bytes() { return sizeof(TSlab) * (size_t)(tcell_threads() / 32); }
 
-int big_warps() { return 148 * 4 * kWarpsPerBlock; } // one slab per resident warp (<= 4 blocks / SM)
+int big_warps() { return 148 * kMaxWarpsPerSM; } // one slab per resident warp
 size_t huge_slab_bytes() { return sizeof(CellMem<kCapHuge, kStackHuge>) * (size_t)kHugeSlabs; }
 size_t big_slab_bytes() { return sizeof(CellMem<kCapBig, kStackBig>) * (size_t)big_warps(); }
 
@@ -1919,11 +1945,11 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
     // (a search radius is not used together with initial guesses)
     void (*kern)(CellArgs);
     if (cl.guesses)
-        kern = k_cells_fast<2, true, false>;
+        kern = k_cells_fast<kMinBlocksLo, true, false>;
     else if (cl.use_hint)
-        kern = cl.min_blocks == 3 ? k_cells_fast<3, false, true> : k_cells_fast<2, false, true>;
+        kern = cl.min_blocks == 3 ? k_cells_fast<kMinBlocksHi, false, true> : k_cells_fast<kMinBlocksLo, false, true>;
     else
-        kern = cl.min_blocks == 3 ? k_cells_fast<3, false, false> : k_cells_fast<2, false, false>;
+        kern = cl.min_blocks == 3 ? k_cells_fast<kMinBlocksHi, false, false> : k_cells_fast<kMinBlocksLo, false, false>;
     int blocks_per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerBlock * 32, 0);
     if (blocks_per_sm < 1)

@@ -30,7 +30,11 @@ constexpr int kStackHuge = 2048;
 constexpr int kHugeSlabs = 256;     // such cells per build (global-memory state each)
 constexpr int kRowWidth = 36;       // row slots per cell: a cell with <= 64 vertices has <= 34 faces
 constexpr int kBigRowWidth = kCapBig; // row slots of a deferred cell
-constexpr int kWarpsPerBlock = 8;   // cell kernel block = 8 warps, one cell per warp at a time
+#ifndef PG_WARPS_PER_BLOCK
+#define PG_WARPS_PER_BLOCK 8
+#endif
+constexpr int kWarpsPerBlock = PG_WARPS_PER_BLOCK; // cell kernel block, one cell per warp at a time
+constexpr int kMaxWarpsPerSM = 32;  // resident cell warps per SM the global slabs are sized for
 constexpr int kMaxLeaf = 32;        // leaf size limit (one candidate per lane)
 constexpr int kDefaultLeaf = 16;
 constexpr int kWindow = 16;         // optional warm start: sorted neighbours i-16 .. i+16
