@@ -244,11 +244,8 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     cl.num_clouds = num_clouds;
     // The reference warm-starts every cell with its kNN(knn) (voronoi_ultra.cu:205-227). The best-first
     // traversal here reaches the seed's own leaf first, which plays that role, so knn does not select
-    // anything; PG_WARM_WINDOW=1 adds a curve-order window warm start for experiments.
-    {
-        const char *ww = std::getenv("PG_WARM_WINDOW");
-        cl.window = (guesses == nullptr && ww && std::atoi(ww) > 0) ? kWindow : 0;
-    }
+    // anything.
+    cl.window = 0;
     cl.guesses = guesses;
     cl.guess_off = guess_off;
     cl.weighted = weights != nullptr;

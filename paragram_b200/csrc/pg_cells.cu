@@ -954,8 +954,6 @@ __device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP
     int first = leaf_first(ref), count = leaf_count(ref);
     int j = first + lane;
     bool have = lane < count && j != i;
-    if (have && !GUESS && A.window > 0 && j >= i - A.window && j <= i + A.window)
-        have = false;
     Cand q;
     float qkey = 0.0f;
     if (have)
@@ -984,14 +982,16 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
                                          float cap, float done_cap, bool &capped)
 {
     const float4 *rec = A.rec;
+    // the root's children; a cloud whose root is a leaf starts with entry -2 (that leaf, unbounded box)
+    const bool root_leaf = ref_is_leaf(ws.root);
     if (lane == 0)
     {
-        m.stk[0] = ws.root << 1;
+        m.stk[0] = root_leaf ? -2 : ws.root << 1;
         m.skey[0] = 0.0f;
         m.stk[1] = (ws.root << 1) | 1;
         m.skey[1] = 0.0f;
     }
-    int sp = 2;
+    int sp = root_leaf ? 1 : 2;
     __syncwarp();
     while (sp > 0)
     {
@@ -1028,20 +1028,31 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
             continue;
         }
         PG_COUNT(m, lane, kStatNodes, 1);
-        int parent = ent >> 1, side = ent & 1;
-        const float4 *r = rec + 4 * (size_t)parent;
-        float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
         float lx, ly, lz, hx, hy, hz, mw;
         int ref;
-        if (side == 0)
+        if (ent < 0)
         {
-            lx = r0.x; ly = r0.y; lz = r0.z; hx = r0.w; hy = r1.x; hz = r1.y; mw = r3.z;
-            ref = __float_as_int(r3.x);
+            // the root leaf of a small cloud: every vertex may be removed by its points
+            lx = ly = lz = -INFINITY;
+            hx = hy = hz = INFINITY;
+            mw = ws.box[6];
+            ref = ws.root;
         }
         else
         {
-            lx = r1.z; ly = r1.w; lz = r2.x; hx = r2.y; hy = r2.z; hz = r2.w; mw = r3.w;
-            ref = __float_as_int(r3.y);
+            int parent = ent >> 1, side = ent & 1;
+            const float4 *r = rec + 4 * (size_t)parent;
+            float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+            if (side == 0)
+            {
+                lx = r0.x; ly = r0.y; lz = r0.z; hx = r0.w; hy = r1.x; hz = r1.y; mw = r3.z;
+                ref = __float_as_int(r3.x);
+            }
+            else
+            {
+                lx = r1.z; ly = r1.w; lz = r2.x; hx = r2.y; hy = r2.z; hz = r2.w; mw = r3.w;
+                ref = __float_as_int(r3.y);
+            }
         }
         if (HINT && ref_is_leaf(ref) && !(key > done_cap))
             continue; // clipped by the first pass
@@ -1153,38 +1164,12 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
                 return;
         }
     }
-    else if (A.window > 0)
-    {
-        int off = lane < A.window ? lane - A.window : lane - A.window + 1;
-        int j = i + off;
-        bool have = lane < 2 * A.window && j >= 0 && j < n;
-        Cand q;
-        float key = 0.0f;
-        if (have)
-        {
-            float4 p = A.pts[j];
-            have = !(p.x == ws.s.x && p.y == ws.s.y && p.z == ws.s.z);
-            q = make_cand(ws.s, p, j);
-            key = q.nrm;
-        }
-        if (!run_batch(m, ws, have, q, key, A, lane, VMask<CAP / 32>{}, false))
-            return;
-    }
     PG_T1(m, lane, kStatCycWarm, tw);
     // 2. BVH traversal, best first (traverse). With a search radius (learned or
     // given), the first pass also drops every node whose bound exceeds it; if
     // the final radius of the cell is within it, the dropped nodes could not
     // clip the cell (certificate), else a second, unbounded pass follows and
     // skips the leaves already clipped.
-    if (ref_is_leaf(ws.root))
-    {
-        VMask<CAP / 32> allv;
-#pragma unroll(CAP > 256 ? 1 : CAP / 32)
-        for (int k = 0; k < CAP / 32; ++k)
-            allv.w[k] = 0xFFFFFFFFu;
-        leaf_batch<CAP, STACK, GUESS>(m, ws, ws.root, i, A, lane, allv);
-        return;
-    }
     float cap = INFINITY, done_cap = -1.0f;
     if (HINT && A.hint != nullptr)
     {
@@ -1344,7 +1329,9 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
         PG_COUNT(m, lane, kStatDeferred, 1);
         if (A.inline_big)
         {
+            PG_T0(tbig);
             big_cell<GUESS>(A, i, lane);
+            PG_T1(m, lane, kStatCycBig, tbig);
             PG_T1(m, lane, kStatCycCell, tcell);
             continue;
         }

@@ -63,7 +63,8 @@ enum Stat : int
     kStatVertex64 = 16,    // vertices rebuilt in FP64 (ill-conditioned in FP32)
     kStatHintHit = 17,     // cells certified within their search radius after the radius dropped a node
     kStatHintMiss = 18,    // cells whose search radius was too small (a second, unbounded pass ran)
-    kNumStats = 19,
+    kStatCycBig = 19,      // SM cycles of the 256/512-slot rebuilds (only with profiling enabled)
+    kNumStats = 20,
 };
 
 // leaf reference encoding in BVH records: bit 31 set, count-1 in bits 26..30,

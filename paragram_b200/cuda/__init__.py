@@ -23,7 +23,7 @@ _LIB = _lib.load()
 #: Counter names returned by ``last_stats()`` (pg_stats in include/paragram_b200.h).
 STAT_NAMES = ["tests", "fp64_escalations", "exact_escalations", "deferred_cells", "nodes", "leaves", "clips",
               "candidates", "cyc_cell", "cyc_warm", "cyc_nodes", "cyc_leaves", "cyc_clips", "cyc_out", "defer_slots",
-              "defer_stack", "vertex64", "hint_hits", "hint_misses"]
+              "defer_stack", "vertex64", "hint_hits", "hint_misses", "cyc_big"]
 _last_stats: dict = {}
 _last_diag: dict = {}
 #: Names of the values returned by ``last_profile()`` (pg_last_profile in include/paragram_b200.h).
