@@ -122,6 +122,8 @@ struct CellArgs
     float *radius_out; // optional per-cell diagnostics (original ids)
     int4 *work_out;
     const float *hint; // search radius per sorted slot (learned or given), or nullptr
+    const int *rparent; // record node -> entry in its parent's record
+    const int *pleaf;   // sorted point -> entry of its leaf
 };
 
 enum Flag : int
@@ -982,16 +984,60 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
                                          float cap, float done_cap, bool &capped)
 {
     const float4 *rec = A.rec;
-    // the root's children; a cloud whose root is a leaf starts with entry -2 (that leaf, unbounded box)
-    const bool root_leaf = ref_is_leaf(ws.root);
-    if (lane == 0)
+    // Start at the seed's own leaf (bound 0) and queue the sibling of every node
+    // on its path up to the cloud's root with its bound, instead of descending
+    // from the root. A cloud whose root is a leaf starts with entry -2 (that
+    // leaf, unbounded box).
+    int sp = 1;
+    if (ref_is_leaf(ws.root))
     {
-        m.stk[0] = root_leaf ? -2 : ws.root << 1;
-        m.skey[0] = 0.0f;
-        m.stk[1] = (ws.root << 1) | 1;
-        m.skey[1] = 0.0f;
+        if (lane == 0)
+        {
+            m.stk[0] = -2;
+            m.skey[0] = 0.0f;
+        }
     }
-    int sp = root_leaf ? 1 : 2;
+    else
+    {
+        int e = A.pleaf[i];
+        if (lane == 0)
+        {
+            m.stk[0] = e;
+            m.skey[0] = 0.0f;
+        }
+        for (int lvl = 0; lvl < STACK - 1; ++lvl)
+        {
+            int parent = e >> 1, side = e & 1;
+            if (e < 0 || parent >= A.n - 1)
+            {
+                ws.flags |= kFlagError; // unreachable: the path always meets the cloud's root
+                break;
+            }
+            const float4 *r = rec + 4 * (size_t)parent;
+            float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+            float k;
+            bool p = side == 1 ? box_key(ws, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r3.z, k)
+                               : box_key(ws, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.w, k);
+            if (HINT)
+            {
+                capped = capped || (p && k > cap);
+                p = p && !(k > cap);
+            }
+            if (p)
+            {
+                if (lane == 0)
+                {
+                    m.stk[sp] = (parent << 1) | (side ^ 1);
+                    m.skey[sp] = k;
+                }
+                ++sp;
+            }
+            if (parent == ws.root)
+                break;
+            e = A.rparent[parent];
+        }
+    }
+    ws.peak = max(ws.peak, sp);
     __syncwarp();
     while (sp > 0)
     {
@@ -1904,6 +1950,8 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.radius_out = cl.radius_out;
     A.work_out = reinterpret_cast<int4 *>(cl.work_out);
     A.hint = cl.use_hint ? ws.hint : nullptr;
+    A.rparent = ws.rparent;
+    A.pleaf = ws.pleaf;
     return A;
 }
 

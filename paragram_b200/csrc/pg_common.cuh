@@ -131,6 +131,8 @@ struct Workspace
     int *flags;           // [N] refit arrival counters
     float4 *nbox;         // [2N] internal node box lo(xyz)+maxw, hi(xyz)+count
     float4 *records;      // [4N] traversal records of internal nodes
+    int *rparent;         // [N] record node -> its entry in its parent's record (parent << 1 | side)
+    int *pleaf;           // [N] sorted point -> the entry of the leaf holding it (parent << 1 | side)
     float *hint;          // [N] search radius per sorted slot (learned or given), <= 0: none
     // cells
     int *rows;            // [N * kRowWidth] directed rows by original index

@@ -373,7 +373,7 @@ __global__ void k_refit(const float4 *__restrict__ pts, int64_t n, const int *__
 //   r3 = (ref0, ref1, maxw0, maxw1)
 __global__ void k_records(const float4 *__restrict__ pts, int64_t n, const int *__restrict__ left,
                           const int *__restrict__ right, const int *__restrict__ first, const float4 *__restrict__ nbox,
-                          int leaf, float4 *__restrict__ rec)
+                          int leaf, float4 *__restrict__ rec, int *__restrict__ rparent, int *__restrict__ pleaf)
 {
     int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ii >= n - 1)
@@ -395,6 +395,12 @@ __global__ void k_records(const float4 *__restrict__ pts, int64_t n, const int *
             cref[c] = leaf_ref(first[x], cnt);
         else
             cref[c] = x;
+        // upward links for traversals that start at a point's own leaf
+        if (cref[c] < 0)
+            for (int p = leaf_first(cref[c]), e = p + leaf_count(cref[c]); p < e; ++p)
+                pleaf[p] = (i << 1) | c;
+        else
+            rparent[x] = (i << 1) | c;
     }
     rec[4 * (size_t)i + 0] = make_float4(clo[0].x, clo[0].y, clo[0].z, chi[0].x);
     rec[4 * (size_t)i + 1] = make_float4(chi[0].y, chi[0].z, clo[1].x, clo[1].y);
@@ -446,7 +452,9 @@ void lbvh_build(const Workspace &ws, int64_t n, int num_clouds, const float *poi
         ++g_launches;
         k_refit<<<g, 256, 0, st>>>(ws.pts, n, ws.left, ws.right, ws.parent_int, ws.parent_leaf, ws.flags, ws.nbox);
         ++g_launches;
-        k_records<<<g, 256, 0, st>>>(ws.pts, n, ws.left, ws.right, ws.first, ws.nbox, leaf_size, ws.records);
+        cudaMemsetAsync(ws.rparent, 0xFF, sizeof(int) * (size_t)n, st); // -1: no parent record
+        k_records<<<g, 256, 0, st>>>(ws.pts, n, ws.left, ws.right, ws.first, ws.nbox, leaf_size, ws.records,
+                                     ws.rparent, ws.pleaf);
     }
     ++g_launches;
     k_cloud_roots<<<(num_clouds + 127) / 128, 128, 0, st>>>(ws.cloud_off, num_clouds, leaf_size, ws.first, ws.last,
