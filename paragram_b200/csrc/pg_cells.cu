@@ -1043,6 +1043,7 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
     {
         PG_T0(tn);
         int jb = sp - 1;
+        float floor_key = 0.0f; // lower bound of every pending bound (best-first only)
         if (sp <= STACK - 64)
         {
             unsigned best = 0xFFFFFFFFu;
@@ -1050,6 +1051,7 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
                 best = min(best, (__float_as_uint(m.skey[j]) & ~(unsigned)(STACK - 1)) | (unsigned)j);
             best = __reduce_min_sync(kFull, best);
             jb = (int)(best & (unsigned)(STACK - 1));
+            floor_key = __uint_as_float(best & ~(unsigned)(STACK - 1));
         }
         // else: a nearly full queue continues depth first (newest entry), which adds at most one
         // pending entry per tree level; the order of visits never changes the cell.
@@ -1066,11 +1068,15 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
         if (key > ws.rsafe)
         {
             PG_T1(m, lane, kStatCycNodes, tn);
+            if (floor_key > ws.rsafe)
+                break; // every pending bound exceeds the radius: the cell is final
             continue;
         }
         if (HINT && key > cap)
         {
             capped = true;
+            if (floor_key > cap)
+                break;
             continue;
         }
         PG_COUNT(m, lane, kStatNodes, 1);
