@@ -617,21 +617,30 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
             for (int e = 0; e < 3; ++e)
                 m.et[(tri_get(t, e) * CAP + tri_get(t, (e + 1) % 3)) >> 5] = 0u;
         }
-    // list the boundary edges by rank in the warp's edge buffer
-    const unsigned lt = (1u << lane) - 1u;
-    int nb = 0;
-#pragma unroll(W > 8 ? 1 : 3 * W)
-    for (int f = 0; f < 3 * W; ++f)
+    // list the boundary edges in the warp's edge buffer, lane by lane (exclusive scan of the counts)
+    int mine = 0;
+    if constexpr (3 * W > 32)
+        mine = __popcll(bf);
+    else
+        mine = __popc((unsigned)bf);
+    int incl = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
     {
-        unsigned bal = __ballot_sync(kFull, (bf >> f) & 1u);
-        if ((bf >> f) & 1u)
-        {
-            unsigned my = tri[f / 3];
-            unsigned x = tri_get(my, f % 3);
-            unsigned y = tri_get(my, (f % 3 + 1) % 3);
-            m.eb[nb + __popc(bal & lt)] = x | (y << 16);
-        }
-        nb += __popc(bal);
+        int v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o)
+            incl += v;
+    }
+    const int nb = __shfl_sync(kFull, incl, 31);
+    {
+        int at = incl - mine;
+#pragma unroll(W > 8 ? 1 : 3 * W)
+        for (int f = 0; f < 3 * W; ++f)
+            if ((bf >> f) & 1u)
+            {
+                unsigned my = tri[f / 3];
+                m.eb[at++] = tri_get(my, f % 3) | (tri_get(my, (f % 3 + 1) % 3) << 16);
+            }
     }
     int nv_new = count_bits(ws.valid) - count_bits(rem) + nb;
     if (nv_new > CAP)
@@ -647,6 +656,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         nbits[k] = 0;
+    bool ill = false; // a vertex built by this lane needs the FP64 rebuild
     // lane r builds the vertex (P, x, y) of the r-th boundary edge in the r-th free slot
     for (int r0 = 0; r0 < nb; r0 += 32)
     {
@@ -669,6 +679,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
             {
                 float vr;
                 float4 X = make_vertex(pP, eP, m.pl[x], m.pe[x], m.pl[y], m.pe[y], vr);
+                ill = ill || !(X.w <= kVertex64Rel * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z)));
                 m.vx[slot] = X;
                 m.vr[slot] = vr;
                 m.vt[slot] = tri_pack((unsigned)P, x, y);
@@ -682,23 +693,26 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         }
     }
     // ill-conditioned in FP32: rebuild in FP64 so that the empty sphere stays tight
-#pragma unroll(CAP > 256 ? 1 : CAP / 32)
-    for (int k = 0; k < W; ++k)
+    if (__any_sync(kFull, ill))
     {
-        unsigned mm = nbits[k];
-        while (mm)
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+        for (int k = 0; k < W; ++k)
         {
-            int slot = k * 32 + __ffs(mm) - 1;
-            mm &= mm - 1;
-            float4 X = m.vx[slot];
-            if (!(X.w <= kVertex64Rel * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z))))
+            unsigned mm = nbits[k];
+            while (mm)
             {
-                unsigned t = m.vt[slot];
-                float vr = m.vr[slot];
-                m.vx[slot] = make_vertex64(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], A.pts, A.oid,
-                                           ws.box, ws.s, X, vr, vr);
-                m.vr[slot] = vr;
-                atomicAdd(&m.cnt[kStatVertex64], 1ull);
+                int slot = k * 32 + __ffs(mm) - 1;
+                mm &= mm - 1;
+                float4 X = m.vx[slot];
+                if (!(X.w <= kVertex64Rel * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z))))
+                {
+                    unsigned t = m.vt[slot];
+                    float vr = m.vr[slot];
+                    m.vx[slot] = make_vertex64(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], A.pts, A.oid,
+                                               ws.box, ws.s, X, vr, vr);
+                    m.vr[slot] = vr;
+                    atomicAdd(&m.cnt[kStatVertex64], 1ull);
+                }
             }
         }
     }
