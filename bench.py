@@ -365,9 +365,18 @@ def run_gpu(args, spec, rank, world, local):
         model, train_info = train_model(dev, rank)
     blob = model.blob if model is not None else None
 
-    def step_device(with_model=True):
-        return pc._run(d_pts, d_w, 8, False, None, None, -1, profile=True,
+    def step_device(with_model=True, profile=False):
+        return pc._run(d_pts, d_w, 8, False, None, None, -1, profile=profile,
                        model=blob if with_model else None)
+
+    def cell_pass_ms(with_model=True):
+        # phase times come from a separate profiled build: the timed steps carry no per-phase events
+        ms = []
+        for _ in range(3):
+            flush.fill_(1.0)
+            step_device(with_model, profile=True)
+            ms.append(pc.last_profile()["cells_ms"])
+        return statistics.median(ms)
 
     host_out = _PinnedOut()
 
@@ -386,8 +395,17 @@ def run_gpu(args, spec, rank, world, local):
     torch.cuda.synchronize(dev)
     dist.barrier()
     with ClockSampler(local) as clocks:
-        times, cell_ms, launches, (adj, off, st) = _timed(step_device, args.steps, dev, flush)
-        plain = _timed(lambda: step_device(False), args.steps, dev, flush) if use_model else None
+        # learned and plain steps interleaved, so that neither gets the warmer half of the run
+        times, cell_ms, launches, plain = [], [], 0, ([], [], 0, None) if use_model else None
+        for _ in range(args.steps):
+            t, c, l_, out = _timed(step_device, 1, dev, flush)
+            times += t
+            cell_ms += c
+            launches += l_
+            (adj, off, st) = out
+            if use_model:
+                pt = _timed(lambda: step_device(False), 1, dev, flush)
+                plain = (plain[0] + pt[0], plain[1] + pt[1], plain[2] + pt[2], pt[3])
     dist.barrier()
     torch.cuda.synchronize(dev)
     total_ms = dist.reduce_max(sum(times), dev)
@@ -407,13 +425,15 @@ def run_gpu(args, spec, rank, world, local):
     e2e_ms = dist.reduce_max(sum(e2e_times), dev)
     e2e_value = total_cells / (e2e_ms / 1e3) / 1e6
     h2d = n * 12 + (n * 4 if h_w is not None else 0)
-    # counters of one more (untimed) build: escalations, fallback rate
+    # counters of one more (untimed) build: escalations, fallback rate; the cell pass alone
     _, cnt = pc.build_with_stats(d_pts, d_w, model=blob)
+    cells_main = cell_pass_ms(True)
+    cells_plain = cell_pass_ms(False) if use_model else None
 
     if rank == 0:
         off_np = off.cpu().numpy()
         flops, nbytes = algorithmic_work(off_np, spec["weighted"])
-        cell_s = statistics.mean(cell_ms) / 1e3
+        cell_s = cells_main / 1e3
         csum = clocks.summary()
         config = {"workload": args.workload, "n_points": n, "weighted": spec["weighted"],
                   "l2": "flushed between steps (256 MiB write)",
@@ -428,7 +448,8 @@ def run_gpu(args, spec, rank, world, local):
             config["learned"] = dict(train_info, fallback_rate=cnt["hint_misses"] / n,
                                      capped_cells=(cnt["hint_hits"] + cnt["hint_misses"]) / n)
             config["plain"] = {"value": plain_value, "unit": "Mcells/s", "ms_per_step": statistics.mean(plain[0]),
-                               "cell_pass_ms": statistics.mean(plain[1])}
+                               "step_ms": [round(t, 2) for t in plain[0]],
+                               "cell_pass_ms": cells_plain}
             config["learned_over_plain"] = value / plain_value if plain_value else None
         line = {
             "metric": "Mcells/s",
@@ -443,6 +464,7 @@ def run_gpu(args, spec, rank, world, local):
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
+            "step_ms": [round(t, 2) for t in times],
             "config": config,
             "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": _roofline(flops, nbytes, cell_s, csum, "k_cells_fast (cell pass)",
