@@ -427,6 +427,16 @@ def run_gpu(args, spec, rank, world, local):
     h2d = n * 12 + (n * 4 if h_w is not None else 0)
     # counters of one more (untimed) build: escalations, fallback rate; the cell pass alone
     _, cnt = pc.build_with_stats(d_pts, d_w, model=blob)
+    fp32_only = None
+    if args.fp32_only_too:
+        # the same build with FP32-only side tests (the reference's arithmetic: no escalation)
+        def step_fp32():
+            return pc._run(d_pts, d_w, 8, False, None, None, -1, fp32_only=True)
+        step_fp32()
+        ft, _, _, (fa, fo, fs) = _timed(step_fp32, args.steps, dev, flush)
+        fv = total_cells / (dist.reduce_max(sum(ft), dev) / 1e3) / 1e6
+        fp32_only = {"value": fv, "unit": "Mcells/s", "ms_per_step": statistics.mean(ft),
+                     "identical_to_exact": bool(torch.equal(fa, adj) and torch.equal(fo, off) and torch.equal(fs, st))}
     cells_main = cell_pass_ms(True)
     cells_plain = cell_pass_ms(False) if use_model else None
 
@@ -443,6 +453,8 @@ def run_gpu(args, spec, rank, world, local):
                                  "fp64_fraction": cnt["fp64_escalations"] / max(cnt["tests"], 1),
                                  "exact_fraction": cnt["exact_escalations"] / max(cnt["tests"], 1),
                                  "fp64_vertices_per_cell": cnt["vertex64"] / n}}
+        if fp32_only is not None:
+            config["fp32_only_predicates"] = fp32_only
         if use_model:
             config["search_radius"] = "learned (MLP 16-64-64-2, BF16, trained before timing)"
             config["learned"] = dict(train_info, fallback_rate=cnt["hint_misses"] / n,
@@ -554,6 +566,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--plain", action="store_true", help="time the plain build only (no learned radius)")
+    ap.add_argument("--fp32-only-too", action="store_true",
+                    help="also time the build with FP32-only side tests (no FP64 / exact escalation)")
     args = ap.parse_args()
     spec = WORKLOADS[args.workload]
     from paragram_b200 import dist

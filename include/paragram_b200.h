@@ -62,7 +62,11 @@ typedef struct pg_options
     int32_t blocks_per_sm; /* register budget of the cell kernel: resident blocks of 8 warps per SM
                               (2 or 3; 0 = default 2). No reference counterpart; chosen by the
                               autotuner. Results do not depend on it. */
-    int32_t reserved;      /* must be 0 */
+    int32_t predicates;    /* 0 (default): FP32 side tests behind a rigorous error filter, undecided ones
+                              re-evaluated in FP64 and exact expansions (exact results). 1: FP32 side
+                              tests only, undecided ones taken by the sign of the FP32 value, as the
+                              reference's FP32 clipping: no escalation, results may differ from the
+                              exact diagram on near-degenerate inputs. */
     const void *model;     /* learned search radius: device pointer to a pg_model, or NULL for the
                               plain traversal. No reference counterpart. Results do not depend on it. */
     const float *radius_hint; /* device float32 [num_points] or NULL: a search radius per point (for

@@ -22,7 +22,7 @@ class PgOptions(ctypes.Structure):
         ("debug", ctypes.c_int32),
         ("num_chunks", ctypes.c_int32),
         ("blocks_per_sm", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("predicates", ctypes.c_int32),
         ("model", ctypes.c_void_p),
         ("radius_hint", ctypes.c_void_p),
         ("radius_out", ctypes.c_void_p),

@@ -194,8 +194,8 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         return fail(PG_ERR_INVALID, "workspace must be 256-byte aligned");
     if (opt.leaf_size > kMaxLeaf)
         return fail(PG_ERR_INVALID, "leaf_size must be at most 32");
-    if (opt.reserved != 0)
-        return fail(PG_ERR_INVALID, "options.reserved must be 0");
+    if (opt.predicates != 0 && opt.predicates != 1)
+        return fail(PG_ERR_INVALID, "options.predicates must be 0 (filtered exact) or 1 (FP32 only)");
     if (((uintptr_t)opt.features_out & 15u) != 0 || ((uintptr_t)opt.model & 15u) != 0)
         return fail(PG_ERR_INVALID, "features_out and model must be 16-byte aligned");
     if (((uintptr_t)opt.work_out & 15u) != 0 || ((uintptr_t)opt.radius_out & 3u) != 0)
@@ -257,6 +257,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         cl.min_blocks = mb ? std::atoi(mb) : (opt.blocks_per_sm == 3 ? 3 : 2);
         cl.big_cap = big_cap(n);
     }
+    cl.fp32_only = opt.predicates == 1;
     cl.radius_out = opt.radius_out;
     cl.work_out = opt.work_out;
     cl.use_hint = 0;

@@ -124,6 +124,7 @@ struct CellArgs
     const float *hint; // search radius per sorted slot (learned or given), or nullptr
     const int *rparent; // record node -> entry in its parent's record
     const int *pleaf;   // sorted point -> entry of its leaf
+    int fp32_only;      // undecided FP32 side tests take the FP32 sign (no exact cascade)
 };
 
 enum Flag : int
@@ -217,6 +218,13 @@ __device__ __forceinline__ int side_fp32(float4 X, const Cand &q)
 
 // Source of plane `pid` (a sorted point index, or -1 - box code) of a cell
 // whose cloud box is `box`.
+// Sign of the FP32 side value alone (1 removed, 0 kept), for FP32-only predicates.
+__device__ __forceinline__ int side_fp32_sign(float4 X, const Cand &q)
+{
+    float g = __fmaf_rn(q.nx, X.x, __fmaf_rn(q.ny, X.y, __fmaf_rn(q.nz, X.z, -q.h)));
+    return g > 0.0f ? 1 : 0;
+}
+
 __device__ __forceinline__ exact::PlaneSrc plane_src(int pid, const float4 *__restrict__ pts,
                                                      const int *__restrict__ oid, const float *__restrict__ box)
 {
@@ -518,6 +526,8 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
             int slot = k * 32 + lane;
             float4 X = m.vx[slot];
             r = side_fp32(X, q);
+            if (r < 0 && A.fp32_only)
+                r = side_fp32_sign(X, q);
             if (r < 0)
             {
                 unsigned t = m.vt[slot];
@@ -1971,6 +1981,7 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.work_out = reinterpret_cast<int4 *>(cl.work_out);
     A.hint = cl.use_hint ? ws.hint : nullptr;
     A.rparent = ws.rparent;
+    A.fp32_only = cl.fp32_only;
     A.pleaf = ws.pleaf;
     return A;
 }

@@ -38,6 +38,7 @@ struct CellLaunch
     float *radius_out; // per original id: certified radius of the final cell, or nullptr
     int *work_out;     // per original id: nodes, leaves, candidates, peak queue; or nullptr
     int use_hint;      // the workspace holds a search radius per sorted slot
+    int fp32_only;     // side tests in FP32 only (no escalation; not exact)
 };
 void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int num_sms, cudaStream_t st);
 void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st);

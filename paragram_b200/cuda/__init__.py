@@ -39,7 +39,7 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
          initial_guesses: Optional[torch.Tensor], initial_guesses_offsets: Optional[torch.Tensor], leaf_size: int,
          num_chunks: int = 0, stats: bool = False, profile: bool = False, blocks_per_sm: int = 0,
          diagnostics: bool = False, model: Optional[torch.Tensor] = None,
-         radius_hint: Optional[torch.Tensor] = None, features: bool = False):
+         radius_hint: Optional[torch.Tensor] = None, features: bool = False, fp32_only: bool = False):
     n = int(points.shape[0])
     _check(points.device.type == "cuda", "points must be on CUDA device")
     _check(points.dtype == torch.float32, "points must be of type float")
@@ -66,6 +66,7 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
         gptr, optr = initial_guesses.data_ptr(), initial_guesses_offsets.data_ptr()
     opts = _lib.PgOptions(int(knn), int(leaf_size), int(bool(debug)) | (2 if profile else 0), int(num_chunks),
                           int(blocks_per_sm))
+    opts.predicates = 1 if fp32_only else 0
     if model is not None:
         _check(model.device == dev and model.dtype == torch.uint8 and model.is_contiguous(),
                "model must be a contiguous uint8 tensor (a packed pg_model) on the points' device")
@@ -142,7 +143,7 @@ def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = Non
                      initial_guesses: Optional[torch.Tensor] = None,
                      initial_guesses_offsets: Optional[torch.Tensor] = None, diagnostics: bool = False,
                      model: Optional[torch.Tensor] = None, radius_hint: Optional[torch.Tensor] = None,
-                     features: bool = False):
+                     features: bool = False, fp32_only: bool = False):
     """Build and return ``((adjacency, offsets, status), counters)``; counters as in ``STAT_NAMES``.
 
     With ``diagnostics=True`` the counters also hold ``radius`` (float32 [N], the certified radius
@@ -150,13 +151,16 @@ def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = Non
     tested, peak node-queue length). ``model`` is a packed learned-radius model (uint8 tensor);
     ``radius_hint`` (float32 [N]) gives a search radius per point instead. With ``features=True``
     the counters also hold ``features`` (float32 [N, 16], the learned model's inputs) and
-    ``order`` (int32 [N], the curve order: sorted slot -> point index).
+    ``order`` (int32 [N], the curve order: sorted slot -> point index). ``fp32_only`` decides every
+    side test by its FP32 value (no FP64 / exact escalation; the result may differ from the exact
+    diagram on near-degenerate input).
     """
     if weights is not None and weights.dim() == 1:
         weights = weights[:, None]
     res = _run(points, weights, knn, False, initial_guesses, initial_guesses_offsets, leaf_size,
                num_chunks=num_chunks, stats=True, profile=profile, blocks_per_sm=blocks_per_sm,
-               diagnostics=diagnostics, model=model, radius_hint=radius_hint, features=features)
+               diagnostics=diagnostics, model=model, radius_hint=radius_hint, features=features,
+               fp32_only=fp32_only)
     out = dict(_last_stats)
     out.update(_last_diag)
     return res, out

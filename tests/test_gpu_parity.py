@@ -284,3 +284,17 @@ def test_radius_hint_never_changes_results(dev, oracle, scale):
             assert st2["hint_misses"] > 0.5 * len(pts)
         if not scale > 0.0:
             assert st2["hint_hits"] + st2["hint_misses"] == 0
+
+
+def test_fp32_only_predicates(dev, oracle):
+    """FP32-only side tests (the reference's arithmetic, no escalation): no FP64 or exact work,
+    and on inputs in general position the same diagram as the exact path."""
+    import paragram_b200.cuda as pc
+    from paragram_b200 import workloads as W
+
+    for pts, w in ((W.uniform(20000, seed=21), None), W.power_uniform(20000, seed=22)):
+        t = torch.from_numpy(pts).to(dev)
+        tw = None if w is None else torch.from_numpy(w).to(dev)
+        (a, o, s), st = pc.build_with_stats(t, tw, fp32_only=True)
+        assert st["fp64_escalations"] == 0 and st["exact_escalations"] == 0
+        _assert_same((a.cpu().numpy(), o.cpu().numpy(), s.cpu().numpy()), oracle.diagram(pts, w), "fp32 only")
