@@ -52,6 +52,7 @@ WORKLOADS = {
     "uniform_power_1m": dict(kind="power", n=1_000_000, weighted=True),
     "lattice_power_310": dict(kind="lattice", n=310 ** 3, weighted=True),
     "surface_batch_256": dict(kind="surfaces", n=256, weighted=False),
+    "surface_cloud_500k": dict(kind="surface", n=500_000, weighted=False),
 }
 #: workloads built with the learned search radius (plain build timed beside them)
 LEARNED = {"clustered_voronoi_5m", "clustered_voronoi_500k"}
@@ -71,6 +72,8 @@ def make_points(spec: dict, seed: int):
         return W.jittered_lattice(round(spec["n"] ** (1 / 3)), seed=seed)
     if k == "surfaces":
         return W.surface_clouds(num_clouds=spec["n"], seed=seed), None
+    if k == "surface":
+        return W.surface_cloud(spec["n"], np.random.default_rng(seed)), None
     raise ValueError(k)
 
 
@@ -375,7 +378,8 @@ def run_gpu(args, spec, rank, world, local):
         for _ in range(3):
             flush.fill_(1.0)
             step_device(with_model, profile=True)
-            ms.append(pc.last_profile()["cells_ms"])
+            pr = pc.last_profile()
+            ms.append(pr["cells_ms"] + pr["deferred_ms"])  # both cell launches
         return statistics.median(ms)
 
     host_out = _PinnedOut()
@@ -425,7 +429,7 @@ def run_gpu(args, spec, rank, world, local):
     e2e_ms = dist.reduce_max(sum(e2e_times), dev)
     e2e_value = total_cells / (e2e_ms / 1e3) / 1e6
     h2d = n * 12 + (n * 4 if h_w is not None else 0)
-    # counters of one more (untimed) build: escalations, fallback rate; the cell pass alone
+    # counters of one more (untimed) build: escalations, fallback rate, traversal work; the cell pass alone
     _, cnt = pc.build_with_stats(d_pts, d_w, model=blob)
     fp32_only = None
     if args.fp32_only_too:
@@ -435,8 +439,10 @@ def run_gpu(args, spec, rank, world, local):
         step_fp32()
         ft, _, _, (fa, fo, fs) = _timed(step_fp32, args.steps, dev, flush)
         fv = total_cells / (dist.reduce_max(sum(ft), dev) / 1e3) / 1e6
+        dd = (fo[1:] - fo[:-1]) != (off[1:] - off[:-1])
         fp32_only = {"value": fv, "unit": "Mcells/s", "ms_per_step": statistics.mean(ft),
-                     "identical_to_exact": bool(torch.equal(fa, adj) and torch.equal(fo, off) and torch.equal(fs, st))}
+                     "identical_to_exact": bool(torch.equal(fa, adj) and torch.equal(fo, off) and torch.equal(fs, st)),
+                     "cells_with_other_degree_or_status": int((dd | (fs != st)).sum())}
     cells_main = cell_pass_ms(True)
     cells_plain = cell_pass_ms(False) if use_model else None
 
@@ -452,7 +458,9 @@ def run_gpu(args, spec, rank, world, local):
                   "escalation": {"fp32_tests_per_cell": cnt["tests"] / n,
                                  "fp64_fraction": cnt["fp64_escalations"] / max(cnt["tests"], 1),
                                  "exact_fraction": cnt["exact_escalations"] / max(cnt["tests"], 1),
-                                 "fp64_vertices_per_cell": cnt["vertex64"] / n}}
+                                 "fp64_vertices_per_cell": cnt["vertex64"] / n},
+                  "work_per_cell": {k: round(cnt[k] / n, 3) for k in ("nodes", "leaves", "candidates", "clips",
+                                                                       "deferred_cells")}}
         if fp32_only is not None:
             config["fp32_only_predicates"] = fp32_only
         if use_model:

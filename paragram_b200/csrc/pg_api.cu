@@ -258,6 +258,13 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         cl.big_cap = big_cap(n);
     }
     cl.fp32_only = opt.predicates == 1;
+    // Cells that outgrow 64 slots are rebuilt with 256 by a second launch over the deferred list:
+    // run inside the first pass, their large code evicts the first pass's from the instruction
+    // cache (surface data: 1% of cells, instruction-fetch stalls 20x). PG_INLINE_BIG=1 keeps them inline.
+    {
+        const char *ib = std::getenv("PG_INLINE_BIG");
+        cl.inline_big = (ib && std::atoi(ib) > 0) ? 1 : 0;
+    }
     cl.radius_out = opt.radius_out;
     cl.work_out = opt.work_out;
     cl.use_hint = 0;
@@ -289,7 +296,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     }
     if (timing)
         cudaEventRecord(ev[4], st);
-    if (cl.min_blocks == 0) // the thread-per-cell variant defers to a separate pass
+    if (cl.min_blocks == 0 || !cl.inline_big) // deferred cells: second launch over the deferred list
         cells_big_launch(ws, cl, status, big_cap(n), st);
     if (timing)
         cudaEventRecord(ev[2], st);

@@ -1391,6 +1391,8 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
                 atomicExch(&A.counters[2], 1);
             ws.flags &= ~kFlagError;
         }
+        if (A.big_pass && (ws.flags & kFlagDefer) && ws.si < A.big_cap && huge_cell(A, i, lane, ws.si))
+            continue; // outgrew the 256 slots too: rebuilt with 512
         if (!(ws.flags & kFlagDefer) || A.big_pass)
         {
             PG_T0(to);
@@ -2020,7 +2022,7 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerBlock * 32, 0);
     if (blocks_per_sm < 1)
         blocks_per_sm = 1;
-    A.inline_big = 1;
+    A.inline_big = cl.inline_big;
     A.big_cap = cl.big_cap;
     int64_t grid = std::min<int64_t>((int64_t)num_sms * blocks_per_sm, big_warps() / kWarpsPerBlock);
     int64_t need = (cells + kWarpsPerBlock - 1) / kWarpsPerBlock;

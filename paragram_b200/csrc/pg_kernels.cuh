@@ -39,6 +39,7 @@ struct CellLaunch
     int *work_out;     // per original id: nodes, leaves, candidates, peak queue; or nullptr
     int use_hint;      // the workspace holds a search radius per sorted slot
     int fp32_only;     // side tests in FP32 only (no escalation; not exact)
+    int inline_big;    // rebuild cells that outgrow 64 slots in the same warp at once (else a second launch)
 };
 void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int num_sms, cudaStream_t st);
 void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st);
