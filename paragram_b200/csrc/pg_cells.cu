@@ -389,9 +389,17 @@ __device__ __forceinline__ void cell_init(CellMem<CAP, STACK> &m, WarpState<CAP>
         int px = sx, py = 2 + sy, pz = 4 + sz;
         int sign = (sx ? 1 : -1) * (sy ? 1 : -1) * (sz ? 1 : -1);
         int p0 = sign > 0 ? px : py, p1 = sign > 0 ? py : px, p2 = pz;
-        float vr;
-        m.vx[lane] = make_vertex(m.pl[p0], m.pe[p0], m.pl[p1], m.pe[p1], m.pl[p2], m.pe[p2], vr);
-        m.vr[lane] = vr;
+        // a corner of the box: each coordinate is a plane offset (n = +-e_axis), exact up to that
+        // offset's own error bound pe; psi as in make_vertex (2 x position bound + FP32 side-test term)
+        float X = sx ? m.pl[px].w : -m.pl[px].w, Y = sy ? m.pl[py].w : -m.pl[py].w,
+              Z = sz ? m.pl[pz].w : -m.pl[pz].w;
+        float ex = (m.pe[px] + m.pe[py] + m.pe[pz]) * (1.0f + 1e-6f);
+        float x2 = X * X + Y * Y + Z * Z;
+        float xn = x2 > 0.0f ? x2 * rsqrtf(x2) * (1.0f + 4e-6f) : 0.0f;
+        float psi = (2.0f * ex + 4.0f * kEps * xn) * (1.0f + 1e-6f);
+        float rr = xn + psi;
+        m.vx[lane] = make_float4(X, Y, Z, psi);
+        m.vr[lane] = rr * rr * (1.0f + 1e-6f);
         m.vt[lane] = tri_pack((unsigned)p0, (unsigned)p1, (unsigned)p2);
     }
     __syncwarp();
