@@ -1,9 +1,10 @@
 """Autotuner for the performance knobs of a workload.
 
 The knobs change speed only, never results (the diagram is exact): the BVH leaf
-size (points per leaf: one candidate batch per warp is at most 32 points), the
-cell kernel's register budget (2 or 3 resident blocks of 8 warps per SM), and
-the number of cell-pass launches. ``tune`` times every combination on a
+size (points per leaf: one candidate batch per warp is at most 32 points) and
+the cell kernel's register budget (2 or 3 resident blocks of 8 warps per SM).
+The number of cell-pass launches is chosen from the free device memory
+(``PARAGRAM_MEM_FRAC``), not timed. ``tune`` times every combination on a
 representative sample on the current GPU and returns the fastest; results are
 cached in memory per (device name, sample signature).
 """

@@ -24,7 +24,6 @@ Typical use::
 
 from __future__ import annotations
 
-import ctypes
 import math
 from dataclasses import dataclass
 from typing import Optional, Sequence
