@@ -8,10 +8,10 @@
 // (pwr_bvh.cuh:217-356).
 //
 // Here one warp owns a cell. The polyhedron lives in shared memory
-// (struct CellMem: planes, vertices, plane ids, traversal stack); lanes own
-// vertex slots (slot = k * 32 + lane). Candidates come in batches of up to 32
-// (one per lane): the warm-start window of curve-order neighbours, the
-// caller's initial guesses, then BVH leaves. A batch is filtered by a
+// (struct CellMem: planes, vertices, plane ids, node queue, edge table); lanes
+// own vertex slots (slot = k * 32 + lane). Candidates come in batches of up to
+// 32 (one per lane): the caller's initial guesses, if any, then BVH leaves,
+// best first from the seed's own leaf. A batch is filtered by a
 // security-radius test, then by an FP32 vertex test with a rigorous error
 // bound; the surviving candidates clip one at a time, nearest first:
 //   1. every lane classifies its vertices (FP32 filter; undecided tests go to
@@ -19,20 +19,22 @@
 //   2. the removed vertices' triangles (in the dual: each vertex is a triangle
 //      of its three planes) give the boundary edges of the new face: a
 //      directed edge x->y of a removed triangle whose reverse is not an edge
-//      of another removed triangle; each boundary edge x->y makes the new
+//      of another removed triangle (found through a per-warp bit table of
+//      the removed triangles' edges); each boundary edge x->y makes the new
 //      vertex (P, x, y) -- the reference builds the same cycle sequentially
 //      in CCComputeBoundary (faster_convex_cell.cuh:322-388);
 //   3. new vertices fill the freed slots (ballot / popc ranks), are computed
 //      in FP32 by Cramer's rule with an a-posteriori error bound (residuals of
-//      the exact planes at the computed point times ||A^-1||).
+//      the exact planes at the computed point, per adjugate column), rebuilt
+//      in FP64 when that bound is large.
 // A BVH node is visited only if some vertex v could be removed by a point of
 // the node's box: dist(v, box)^2 < |v - s|^2 + (max weight in box - w_s),
 // tested lane-parallel over the vertices.
 //
-// A cell that needs more than 64 vertex / plane slots or 64 stack entries is
-// deferred to a second pass with 256 slots in global memory; its status is
+// A cell that needs more than 64 vertex / plane slots is deferred to a second
+// launch with 256 slots in global memory (then 512 if needed); its status is
 // then vertex_overflow (2) if the final cell has more than 64 vertices (the
-// reference MAX_VERTS) and plane_overflow (1) only if even 256 slots overflow.
+// reference MAX_VERTS) and plane_overflow (1) only if even 512 slots overflow.
 #include <cfloat>
 #include <climits>
 #include <type_traits>
