@@ -82,6 +82,10 @@ typedef struct pg_options
                               the learned search radius (training inputs; pg_model below). */
     int32_t *order_out;    /* device int32 [num_points] or NULL: the points' curve order (sorted slot
                               -> point index) used by the BVH and by the features' windows. */
+    float *geometry_out;   /* device float32 [4 * num_points], 16-byte aligned, or NULL: per point, the
+                              centroid (x, y, z) and the volume of its cell (the geometry the reference
+                              computes and discards, voronoi_ultra.cu:125-138). An empty cell gives
+                              volume 0 and a NaN centroid; a plane_overflow cell NaN. */
 } pg_options;
 
 /* Learned search radius (no reference counterpart). A 16 -> 64 -> 64 -> 2 MLP

@@ -8,10 +8,12 @@ fallback -- calling the API without the built library raises ImportError.
 
 from ._api import Diagram, power_diagram, voronoi_diagram
 from .batch import build_batch
+from .geometry import cell_geometry
 
 __all__ = [
     "Diagram",
     "build_batch",
+    "cell_geometry",
     "power_diagram",
     "voronoi_diagram",
 ]

@@ -29,6 +29,7 @@ class PgOptions(ctypes.Structure):
         ("work_out", ctypes.c_void_p),
         ("features_out", ctypes.c_void_p),
         ("order_out", ctypes.c_void_p),
+        ("geometry_out", ctypes.c_void_p),
     ]
 
 

@@ -178,7 +178,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
 {
     g_last_error.clear();
     cudaStream_t st = (cudaStream_t)stream;
-    pg_options opt = {8, -1, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    pg_options opt = {8, -1, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
     if (options)
         opt = *options;
     const bool sync = num_edges != nullptr;
@@ -200,6 +200,8 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         return fail(PG_ERR_INVALID, "features_out and model must be 16-byte aligned");
     if (((uintptr_t)opt.work_out & 15u) != 0 || ((uintptr_t)opt.radius_out & 3u) != 0)
         return fail(PG_ERR_INVALID, "work_out must be 16-byte and radius_out 4-byte aligned");
+    if (((uintptr_t)opt.geometry_out & 15u) != 0)
+        return fail(PG_ERR_INVALID, "geometry_out must be 16-byte aligned");
     size_t need = workspace_layout(n, num_clouds, nullptr, nullptr);
     if (workspace_bytes < need)
         return fail(PG_ERR_INVALID, "workspace too small: need " + std::to_string(need) + " bytes");
@@ -267,6 +269,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     }
     cl.radius_out = opt.radius_out;
     cl.work_out = opt.work_out;
+    cl.geometry_out = opt.geometry_out;
     cl.use_hint = 0;
     if (opt.features_out != nullptr)
         features_launch(ws, n, num_clouds, opt.features_out, st);
@@ -357,7 +360,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
 
 extern "C" {
 
-int pg_version(void) { return 101; }
+int pg_version(void) { return 102; }
 
 const char *pg_last_error(void) { return pg::g_last_error.c_str(); }
 

@@ -123,6 +123,7 @@ struct CellArgs
     int inline_big; // rebuild deferred cells right away in the same kernel (warp path)
     float *radius_out; // optional per-cell diagnostics (original ids)
     int4 *work_out;
+    float4 *geometry_out; // optional per-cell centroid and volume (original ids)
     const float *hint; // search radius per sorted slot (learned or given), or nullptr
     const int *rparent; // record node -> entry in its parent's record
     const int *pleaf;   // sorted point -> entry of its leaf
@@ -1283,10 +1284,161 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
 
 
 // Optional per-cell diagnostics: certified radius and traversal work.
+// Volume and centroid of the final cell (the cell's geometry, which the
+// reference computes and discards: voronoi_ultra.cu:125-138). Each face a is
+// fanned from the foot f_a of the perpendicular from an apex o onto its plane,
+// so the cell is the signed union of the tetrahedra (o, f_a, v_t, v_u) over
+// the directed edges v_t -> v_u of its faces. The vertex triangles are
+// oriented consistently (each plane pair appears once in each direction), so
+// the edge of face a that leaves vertex t = (a, b, c) ends at the vertex whose
+// triangle holds the directed pair a -> c, and all terms share one sign.
+// Writes (centroid x, y, z, volume); a deferred cell writes NaN (the larger
+// pass overwrites it), an empty cell volume 0 and a NaN centroid.
 template <int CAP, int STACK>
-__device__ __forceinline__ void write_diagnostics(const CellMem<CAP, STACK> &m, const WarpState<CAP> &ws,
+__device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const WarpState<CAP> &ws,
+                                               const CellArgs &A, int lane)
+{
+    constexpr int W = WarpState<CAP>::W;
+    if (ws.flags & (kFlagDefer | kFlagEmpty))
+    {
+        if (lane == 0)
+        {
+            float nan = __int_as_float(0x7fc00000);
+            A.geometry_out[ws.soid] = make_float4(nan, nan, nan, (ws.flags & kFlagDefer) ? nan : 0.0f);
+        }
+        return;
+    }
+    // the directed plane pair (a -> c) that each of this lane's vertices needs, per rotation
+    unsigned want[W][3];
+    int succ[W][3];
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+    {
+        unsigned t = m.vt[k * 32 + lane];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+        {
+            want[k][r] = ((ws.valid[k] >> lane) & 1u) ? (tri_get(t, r) << 10 | tri_get(t, (r + 2) % 3)) : ~0u;
+            succ[k][r] = -1;
+        }
+    }
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int kj = 0; kj < W; ++kj)
+    {
+        unsigned vm = ws.valid[kj];
+        while (vm)
+        {
+            int j = kj * 32 + __ffs(vm) - 1;
+            vm &= vm - 1;
+            unsigned tj = m.vt[j];
+            unsigned x0 = tri_get(tj, 0), x1 = tri_get(tj, 1), x2 = tri_get(tj, 2);
+            unsigned e0 = x0 << 10 | x1, e1 = x1 << 10 | x2, e2 = x2 << 10 | x0;
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+            for (int k = 0; k < W; ++k)
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                    if (want[k][r] == e0 || want[k][r] == e1 || want[k][r] == e2)
+                        succ[k][r] = j;
+        }
+    }
+    // The FP32 vertices are only as accurate as the side tests need (psi); rebuild in FP64 the
+    // ones whose bound exceeds 32 ulps of their size, so that each vertex is within about
+    // 2^-19 |v| of the exact one (a power cell far from its seed amplifies that by |v| / size).
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+        if ((ws.valid[k] >> lane) & 1u)
+        {
+            int slot = k * 32 + lane;
+            float4 X = m.vx[slot];
+            if (!(X.w <= 32.0f * kEps * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z))))
+            {
+                unsigned t = m.vt[slot];
+                float vr = m.vr[slot];
+                m.vx[slot] = make_vertex64(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], A.pts,
+                                           A.oid, ws.box, ws.s, X, vr, vr);
+            }
+        }
+    __syncwarp();
+    // apex: the mean vertex (inside the cell), not the seed, which a power cell may lie far from;
+    // tetrahedra from a distant apex would cancel to the cell's small volume
+    float ox = 0.0f, oy = 0.0f, oz = 0.0f, on = 0.0f;
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+        if ((ws.valid[k] >> lane) & 1u)
+        {
+            float4 v = m.vx[k * 32 + lane];
+            ox += v.x;
+            oy += v.y;
+            oz += v.z;
+            on += 1.0f;
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        ox += __shfl_xor_sync(kFull, ox, o);
+        oy += __shfl_xor_sync(kFull, oy, o);
+        oz += __shfl_xor_sync(kFull, oz, o);
+        on += __shfl_xor_sync(kFull, on, o);
+    }
+    ox /= on;
+    oy /= on;
+    oz /= on;
+    float S = 0.0f, cx = 0.0f, cy = 0.0f, cz = 0.0f;
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+    {
+        if (!((ws.valid[k] >> lane) & 1u))
+            continue;
+        int slot = k * 32 + lane;
+        unsigned t = m.vt[slot];
+        float4 v = m.vx[slot];
+        v.x -= ox;
+        v.y -= oy;
+        v.z -= oz;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+        {
+            if (succ[k][r] < 0)
+                continue;
+            float4 p = m.pl[tri_get(t, r)];
+            float4 u = m.vx[succ[k][r]];
+            u.x -= ox;
+            u.y -= oy;
+            u.z -= oz;
+            // foot of the perpendicular from the apex onto the plane n.x <= h
+            float sc = (p.w - (p.x * ox + p.y * oy + p.z * oz)) / (p.x * p.x + p.y * p.y + p.z * p.z);
+            float fx = p.x * sc, fy = p.y * sc, fz = p.z * sc;
+            float d = fx * (v.y * u.z - v.z * u.y) + fy * (v.z * u.x - v.x * u.z) + fz * (v.x * u.y - v.y * u.x);
+            S += d;
+            cx += d * (fx + v.x + u.x);
+            cy += d * (fy + v.y + u.y);
+            cz += d * (fz + v.z + u.z);
+        }
+    }
+    double dS = S, dx = cx, dy = cy, dz = cz;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        dS += __shfl_xor_sync(kFull, dS, o);
+        dx += __shfl_xor_sync(kFull, dx, o);
+        dy += __shfl_xor_sync(kFull, dy, o);
+        dz += __shfl_xor_sync(kFull, dz, o);
+    }
+    if (lane == 0)
+    {
+        double q = 0.25 / dS;
+        A.geometry_out[ws.soid] =
+            make_float4((float)((double)ws.s.x + (double)ox + dx * q), (float)((double)ws.s.y + (double)oy + dy * q),
+                        (float)((double)ws.s.z + (double)oz + dz * q), (float)(fabs(dS) / 6.0));
+    }
+}
+
+template <int CAP, int STACK>
+__device__ __forceinline__ void write_diagnostics(CellMem<CAP, STACK> &m, const WarpState<CAP> &ws,
                                                   const CellArgs &A, int lane)
 {
+    if (A.geometry_out != nullptr)
+        write_geometry(m, ws, A, lane);
     if (lane != 0)
         return;
     if (A.radius_out != nullptr)
@@ -1991,6 +2143,7 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.inline_big = 0;
     A.radius_out = cl.radius_out;
     A.work_out = reinterpret_cast<int4 *>(cl.work_out);
+    A.geometry_out = reinterpret_cast<float4 *>(cl.geometry_out);
     A.hint = cl.use_hint ? ws.hint : nullptr;
     A.rparent = ws.rparent;
     A.fp32_only = cl.fp32_only;

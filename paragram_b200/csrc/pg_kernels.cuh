@@ -37,6 +37,7 @@ struct CellLaunch
     int64_t big_cap; // deferred-row slots
     float *radius_out; // per original id: certified radius of the final cell, or nullptr
     int *work_out;     // per original id: nodes, leaves, candidates, peak queue; or nullptr
+    float *geometry_out; // per original id: centroid x, y, z and volume of the cell; or nullptr
     int use_hint;      // the workspace holds a search radius per sorted slot
     int fp32_only;     // side tests in FP32 only (no escalation; not exact)
     int inline_big;    // rebuild cells that outgrow 64 slots in the same warp at once (else a second launch)

@@ -39,7 +39,8 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
          initial_guesses: Optional[torch.Tensor], initial_guesses_offsets: Optional[torch.Tensor], leaf_size: int,
          num_chunks: int = 0, stats: bool = False, profile: bool = False, blocks_per_sm: int = 0,
          diagnostics: bool = False, model: Optional[torch.Tensor] = None,
-         radius_hint: Optional[torch.Tensor] = None, features: bool = False, fp32_only: bool = False):
+         radius_hint: Optional[torch.Tensor] = None, features: bool = False, fp32_only: bool = False,
+         geometry: bool = False):
     n = int(points.shape[0])
     _check(points.device.type == "cuda", "points must be on CUDA device")
     _check(points.dtype == torch.float32, "points must be of type float")
@@ -85,6 +86,10 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
         feats = torch.zeros(max(n, 1), 16, dtype=torch.float32, device=dev)
         order = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
         opts.features_out, opts.order_out = feats.data_ptr(), order.data_ptr()
+    geom = None
+    if geometry:
+        geom = torch.zeros(max(n, 1), 4, dtype=torch.float32, device=dev)
+        opts.geometry_out = geom.data_ptr()
     with torch.cuda.device(dev):
         nbytes = ctypes.c_size_t(0)
         rc = _LIB.pg_workspace_size(n, ctypes.byref(nbytes))
@@ -114,6 +119,8 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
         _last_diag.update(radius=radius[:n], work=work[:n])
     if features:
         _last_diag.update(features=feats[:n], order=order[:n])
+    if geometry:
+        _last_diag.update(centroids=geom[:n, :3], volumes=geom[:n, 3])
     return adjacency, offsets, status
 
 
@@ -143,7 +150,7 @@ def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = Non
                      initial_guesses: Optional[torch.Tensor] = None,
                      initial_guesses_offsets: Optional[torch.Tensor] = None, diagnostics: bool = False,
                      model: Optional[torch.Tensor] = None, radius_hint: Optional[torch.Tensor] = None,
-                     features: bool = False, fp32_only: bool = False):
+                     features: bool = False, fp32_only: bool = False, geometry: bool = False):
     """Build and return ``((adjacency, offsets, status), counters)``; counters as in ``STAT_NAMES``.
 
     With ``diagnostics=True`` the counters also hold ``radius`` (float32 [N], the certified radius
@@ -153,14 +160,15 @@ def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = Non
     the counters also hold ``features`` (float32 [N, 16], the learned model's inputs) and
     ``order`` (int32 [N], the curve order: sorted slot -> point index). ``fp32_only`` decides every
     side test by its FP32 value (no FP64 / exact escalation; the result may differ from the exact
-    diagram on near-degenerate input).
+    diagram on near-degenerate input). With ``geometry=True`` the counters also hold ``centroids``
+    (float32 [N, 3]) and ``volumes`` (float32 [N]) of the cells (empty cell: volume 0, NaN centroid).
     """
     if weights is not None and weights.dim() == 1:
         weights = weights[:, None]
     res = _run(points, weights, knn, False, initial_guesses, initial_guesses_offsets, leaf_size,
                num_chunks=num_chunks, stats=True, profile=profile, blocks_per_sm=blocks_per_sm,
                diagnostics=diagnostics, model=model, radius_hint=radius_hint, features=features,
-               fp32_only=fp32_only)
+               fp32_only=fp32_only, geometry=geometry)
     out = dict(_last_stats)
     out.update(_last_diag)
     return res, out
