@@ -62,6 +62,10 @@ def test_build_rejects_bad_arguments(lib):
     assert _build(lib, 10, ws_bytes=16) == -1  # workspace too small
     assert _build(lib, 10, options=_lib.PgOptions(8, 64, 0, 0)) == -1  # leaf too large
     assert "leaf_size" in _lib.last_error(lib)
+    opt = _lib.PgOptions(8, -1, 0, 0)
+    opt.geometry_out = 264  # centroid + volume rows need 16-byte alignment
+    assert _build(lib, 10, options=opt) == -1
+    assert "geometry_out" in _lib.last_error(lib)
 
 
 def test_emit_rejects_bad_arguments(lib):
