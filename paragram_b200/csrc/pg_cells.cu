@@ -1284,6 +1284,34 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
 
 
 // Optional per-cell diagnostics: certified radius and traversal work.
+// The vertex of three planes solved in FP64 from the planes' sources (the
+// bisector coefficients are exact differences of FP32 values), without the
+// error bound of make_vertex64: a vertex of the cell geometry. Returns X
+// unchanged when the planes do not give exact FP64 rows or a usable solve.
+__device__ __noinline__ float4 vertex64_plain(int pid0, int pid1, int pid2, const float4 *__restrict__ pts,
+                                              const int *__restrict__ oid, const float *__restrict__ box, float4 s,
+                                              float4 X)
+{
+    exact::DRow r[3];
+    exact::make_drow(plane_src(pid0, pts, oid, box), s.x, s.y, s.z, s.w, r[0]);
+    exact::make_drow(plane_src(pid1, pts, oid, box), s.x, s.y, s.z, s.w, r[1]);
+    exact::make_drow(plane_src(pid2, pts, oid, box), s.x, s.y, s.z, s.w, r[2]);
+    if (!(r[0].ok && r[1].ok && r[2].ok))
+        return X;
+    const double *a = r[0].a, *b = r[1].a, *c = r[2].a;
+    double u0x = b[1] * c[2] - b[2] * c[1], u0y = b[2] * c[0] - b[0] * c[2], u0z = b[0] * c[1] - b[1] * c[0];
+    double u1x = c[1] * a[2] - c[2] * a[1], u1y = c[2] * a[0] - c[0] * a[2], u1z = c[0] * a[1] - c[1] * a[0];
+    double u2x = a[1] * b[2] - a[2] * b[1], u2y = a[2] * b[0] - a[0] * b[2], u2z = a[0] * b[1] - a[1] * b[0];
+    double D = a[0] * u0x + a[1] * u0y + a[2] * u0z;
+    if (!(fabs(D) > 0.0))
+        return X;
+    double q = 0.5 / D;
+    double x = (r[0].b * u0x + r[1].b * u1x + r[2].b * u2x) * q;
+    double y = (r[0].b * u0y + r[1].b * u1y + r[2].b * u2y) * q;
+    double z = (r[0].b * u0z + r[1].b * u1z + r[2].b * u2z) * q;
+    return make_float4((float)x, (float)y, (float)z, X.w);
+}
+
 // Volume and centroid of the final cell (the cell's geometry, which the
 // reference computes and discards: voronoi_ultra.cu:125-138). Each face a is
 // fanned from the foot f_a of the perpendicular from an apex o onto its plane,
@@ -1353,9 +1381,8 @@ __device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const War
             if (!(X.w <= 32.0f * kEps * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z))))
             {
                 unsigned t = m.vt[slot];
-                float vr = m.vr[slot];
-                m.vx[slot] = make_vertex64(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], A.pts,
-                                           A.oid, ws.box, ws.s, X, vr, vr);
+                m.vx[slot] = vertex64_plain(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], A.pts,
+                                            A.oid, ws.box, ws.s, X);
             }
         }
     __syncwarp();
