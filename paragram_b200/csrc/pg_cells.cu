@@ -35,6 +35,10 @@
 // launch with 256 slots in global memory (then 512 if needed); its status is
 // then vertex_overflow (2) if the final cell has more than 64 vertices (the
 // reference MAX_VERTS) and plane_overflow (1) only if even 512 slots overflow.
+//
+// With a geometry output, each final cell is also integrated before it is
+// discarded (integrate_cell: volume and centroid from a fan of signed
+// tetrahedra per face).
 #include <cfloat>
 #include <climits>
 #include <type_traits>
@@ -1322,20 +1326,17 @@ __device__ __noinline__ float4 vertex64_plain(int pid0, int pid1, int pid2, cons
 // triangle holds the directed pair a -> c, and all terms share one sign.
 // Writes (centroid x, y, z, volume); a deferred cell writes NaN (the larger
 // pass overwrites it), an empty cell volume 0 and a NaN centroid.
+// (not inlined: the cell kernels keep their register allocation when no geometry is asked for;
+// the valid-slot masks arrive in m.eb, free once the cell is final)
 template <int CAP, int STACK>
-__device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const WarpState<CAP> &ws,
-                                               const CellArgs &A, int lane)
+__device__ __noinline__ void integrate_cell(CellMem<CAP, STACK> &m, const CellArgs &A, int lane, int soid, float4 s,
+                                            const float *box)
 {
     constexpr int W = WarpState<CAP>::W;
-    if (ws.flags & (kFlagDefer | kFlagEmpty))
-    {
-        if (lane == 0)
-        {
-            float nan = __int_as_float(0x7fc00000);
-            A.geometry_out[ws.soid] = make_float4(nan, nan, nan, (ws.flags & kFlagDefer) ? nan : 0.0f);
-        }
-        return;
-    }
+    unsigned valid[W];
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+        valid[k] = m.eb[k];
     // the directed plane pair (a -> c) that each of this lane's vertices needs, per rotation
     unsigned want[W][3];
     int succ[W][3];
@@ -1346,14 +1347,14 @@ __device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const War
 #pragma unroll
         for (int r = 0; r < 3; ++r)
         {
-            want[k][r] = ((ws.valid[k] >> lane) & 1u) ? (tri_get(t, r) << 10 | tri_get(t, (r + 2) % 3)) : ~0u;
+            want[k][r] = ((valid[k] >> lane) & 1u) ? (tri_get(t, r) << 10 | tri_get(t, (r + 2) % 3)) : ~0u;
             succ[k][r] = -1;
         }
     }
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int kj = 0; kj < W; ++kj)
     {
-        unsigned vm = ws.valid[kj];
+        unsigned vm = valid[kj];
         while (vm)
         {
             int j = kj * 32 + __ffs(vm) - 1;
@@ -1374,7 +1375,7 @@ __device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const War
     // 2^-19 |v| of the exact one (a power cell far from its seed amplifies that by |v| / size).
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
-        if ((ws.valid[k] >> lane) & 1u)
+        if ((valid[k] >> lane) & 1u)
         {
             int slot = k * 32 + lane;
             float4 X = m.vx[slot];
@@ -1382,7 +1383,7 @@ __device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const War
             {
                 unsigned t = m.vt[slot];
                 m.vx[slot] = vertex64_plain(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], A.pts,
-                                            A.oid, ws.box, ws.s, X);
+                                            A.oid, box, s, X);
             }
         }
     __syncwarp();
@@ -1391,7 +1392,7 @@ __device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const War
     float ox = 0.0f, oy = 0.0f, oz = 0.0f, on = 0.0f;
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
-        if ((ws.valid[k] >> lane) & 1u)
+        if ((valid[k] >> lane) & 1u)
         {
             float4 v = m.vx[k * 32 + lane];
             ox += v.x;
@@ -1414,7 +1415,7 @@ __device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const War
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
     {
-        if (!((ws.valid[k] >> lane) & 1u))
+        if (!((valid[k] >> lane) & 1u))
             continue;
         int slot = k * 32 + lane;
         unsigned t = m.vt[slot];
@@ -1454,10 +1455,34 @@ __device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const War
     if (lane == 0)
     {
         double q = 0.25 / dS;
-        A.geometry_out[ws.soid] =
-            make_float4((float)((double)ws.s.x + (double)ox + dx * q), (float)((double)ws.s.y + (double)oy + dy * q),
-                        (float)((double)ws.s.z + (double)oz + dz * q), (float)(fabs(dS) / 6.0));
+        A.geometry_out[soid] =
+            make_float4((float)((double)s.x + (double)ox + dx * q), (float)((double)s.y + (double)oy + dy * q),
+                        (float)((double)s.z + (double)oz + dz * q), (float)(fabs(dS) / 6.0));
     }
+}
+
+template <int CAP, int STACK>
+__device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const WarpState<CAP> &ws,
+                                               const CellArgs &A, int lane)
+{
+    constexpr int W = WarpState<CAP>::W;
+    if (ws.flags & (kFlagDefer | kFlagEmpty))
+    {
+        if (lane == 0)
+        {
+            float nan = __int_as_float(0x7fc00000);
+            A.geometry_out[ws.soid] = make_float4(nan, nan, nan, (ws.flags & kFlagDefer) ? nan : 0.0f);
+        }
+        return;
+    }
+    if (lane == 0)
+    {
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+        for (int k = 0; k < W; ++k)
+            m.eb[k] = ws.valid[k];
+    }
+    __syncwarp();
+    integrate_cell(m, A, lane, ws.soid, ws.s, ws.box);
 }
 
 template <int CAP, int STACK>
