@@ -218,7 +218,10 @@ int pg_mlp_pack(const float *params, void *model, void *stream);
  * PG_ERR_INVALID. The first call on a device resolves the array's address
  * (cudaGetSymbolAddress) with that device current; make that first call before
  * any stream capture. All calls on a device share the array: calls that
- * overlap on the GPU race and must be serialised by the caller. */
+ * overlap on the GPU race and must be serialised by the caller. The resolved
+ * address is kept per device ordinal for the life of the process: after a
+ * cudaDeviceReset (or a new primary context) on that device it is stale, so a
+ * caller that resets a device must not call this entry point afterwards. */
 int pg_degrees_to_offsets_noalloc(int64_t num_rows, const int32_t *degrees, int32_t *offsets, void *stream);
 
 #ifdef __cplusplus

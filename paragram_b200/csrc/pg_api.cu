@@ -82,7 +82,6 @@ size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
     w.big_rows = (int *)take(4 * (size_t)big_cap((int64_t)N) * kBigRowWidth);
     w.big_slabs = take(big_slab_bytes());
     w.huge_slabs = take(huge_slab_bytes());
-    w.tslabs = take(tcell_slab_bytes());
     w.cnt = (int *)take(4 * N);
     w.miss = (int *)take(4 * N);
     w.fill = (int *)take(4 * N);
@@ -253,20 +252,9 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     cl.guesses = guesses;
     cl.guess_off = guess_off;
     cl.weighted = weights != nullptr;
-    {
-        // warp per cell with 2 (default) or 3 blocks per SM; PG_CELL_MIN_BLOCKS=0 selects thread per cell
-        const char *mb = std::getenv("PG_CELL_MIN_BLOCKS");
-        cl.min_blocks = mb ? std::atoi(mb) : (opt.blocks_per_sm == 3 ? 3 : 2);
-        cl.big_cap = big_cap(n);
-    }
+    cl.min_blocks = opt.blocks_per_sm == 3 ? 3 : 2; // register budget of the cell kernel
+    cl.big_cap = big_cap(n);
     cl.fp32_only = opt.predicates == 1;
-    // Cells that outgrow 64 slots are rebuilt with 256 by a second launch over the deferred list:
-    // run inside the first pass, their large code evicts the first pass's from the instruction
-    // cache (surface data: 1% of cells, instruction-fetch stalls 20x). PG_INLINE_BIG=1 keeps them inline.
-    {
-        const char *ib = std::getenv("PG_INLINE_BIG");
-        cl.inline_big = (ib && std::atoi(ib) > 0) ? 1 : 0;
-    }
     cl.radius_out = opt.radius_out;
     cl.work_out = opt.work_out;
     cl.geometry_out = opt.geometry_out;
@@ -299,8 +287,9 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     }
     if (timing)
         cudaEventRecord(ev[4], st);
-    if (cl.min_blocks == 0 || !cl.inline_big) // deferred cells: second launch over the deferred list
-        cells_big_launch(ws, cl, status, big_cap(n), st);
+    // Cells that outgrew 64 slots: a second launch over the deferred list. Rebuilt inside the first
+    // launch, their large code evicted the first pass's from the instruction cache (surface data).
+    cells_big_launch(ws, cl, status, big_cap(n), st);
     if (timing)
         cudaEventRecord(ev[2], st);
     csr_count(ws, n, offsets, st);

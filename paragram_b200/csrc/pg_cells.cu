@@ -124,7 +124,6 @@ struct CellArgs
     int64_t big_cap;
     char *slabs;
     char *huge_slabs;
-    int inline_big; // rebuild deferred cells right away in the same kernel (warp path)
     float *radius_out; // optional per-cell diagnostics (original ids)
     int4 *work_out;
     float4 *geometry_out; // optional per-cell centroid and volume (original ids)
@@ -1536,46 +1535,6 @@ __device__ __noinline__ bool huge_cell(const CellArgs &A, int i, int lane, int s
     return true;
 }
 
-// Rebuild cell i with 256 vertex / plane slots and a 1024-entry queue in this
-// warp's global slab. Called by the warp whose shared-memory cell outgrew its
-// 64 slots, right away, so that the few expensive cells overlap with the rest
-// of the cell pass instead of forming a tail after it. A cell that outgrows the
-// 256 slots too is rebuilt once more by huge_cell.
-template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, int i, int lane)
-{
-    size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    auto &m = *reinterpret_cast<CellMem<kCapBig, kStackBig> *>(A.slabs + gw * sizeof(CellMem<kCapBig, kStackBig>));
-    WarpState<kCapBig> ws;
-    if (lane < kNumStats)
-        m.cnt[lane] = 0;
-    int slot = 0;
-    if (lane == 0)
-        slot = atomicAdd(&A.counters[1], 1);
-    slot = __shfl_sync(kFull, slot, 0);
-    clear_edges(m, lane);
-    process_cell<kCapBig, kStackBig, GUESS, false>(m, ws, i, A, lane);
-    write_diagnostics(m, ws, A, lane);
-    if ((ws.flags & kFlagError) && lane == 0)
-        atomicExch(&A.counters[2], 1);
-    if ((ws.flags & kFlagDefer) && slot < A.big_cap && huge_cell(A, i, lane, slot))
-    {
-        flush_stats(m, A, lane);
-        return;
-    }
-    if (slot < A.big_cap)
-    {
-        ws.si = slot; // deferred-row slot
-        write_outputs(m, ws, A, lane, true);
-    }
-    else if (lane == 0)
-    {
-        // out of deferred-row slots: reported by the host as an error
-        A.deg[ws.soid] = 0;
-        A.status[ws.soid] = kPlaneOverflow;
-    }
-    flush_stats(m, A, lane);
-}
-
 template <int CAP, int STACK, bool GUESS, bool HINT>
 __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArgs &A, int lane)
 {
@@ -1619,14 +1578,6 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
             }
         }
         PG_COUNT(m, lane, kStatDeferred, 1);
-        if (A.inline_big)
-        {
-            PG_T0(tbig);
-            big_cell<GUESS>(A, i, lane);
-            PG_T1(m, lane, kStatCycBig, tbig);
-            PG_T1(m, lane, kStatCycCell, tcell);
-            continue;
-        }
         // deferred: placeholder outputs (an empty row) until the large-capacity pass
         if (lane == 0)
         {
@@ -1654,511 +1605,6 @@ template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_c
     auto *m = reinterpret_cast<CellMem<kCapBig, kStackBig> *>(A.slabs + gw * sizeof(CellMem<kCapBig, kStackBig>));
     cells_body<kCapBig, kStackBig, GUESS, false>(*m, A, lane);
 }
-
-// ===========================================================================
-// Thread-per-cell fast path.
-//
-// One thread owns a cell (the reference's decomposition, voronoi_ultra.cu:51),
-// so a warp advances 32 neighbouring cells (curve order) at once. The cell
-// lives in a per-warp slab of global memory laid out [slot][lane] (a warp's
-// 32 threads touching the same slot read 32 consecutive elements), cached in
-// L1. The polyhedron is kept compact: vertices [0, nv), planes [0, np).
-// Node and point pruning use the directional corner radius of the cell's
-// conservative bounding box (the reference's get_directional_safety_radius,
-// voronoi_bvh.cuh:71-107, here with rounding margins so that it never prunes
-// a point that could remove a vertex). Cells that need more than kTCap
-// slots or kTStack stack entries are deferred to the 256-slot warp pass.
-// ===========================================================================
-constexpr int kTCap = 64;
-constexpr int kTStack = 64;
-constexpr int kTMaxBoundary = 48;
-
-struct TSlab
-{
-    float4 pl[kTCap][32];
-    float4 vx[kTCap][32];
-    float pe[kTCap][32];
-    int pid[kTCap][32];
-    unsigned vt[kTCap][32];
-};
-
-struct TCell
-{
-    float4 s;
-    int si, soid;
-    const float *box;
-    int root;
-    int nv, np;
-    float lx, ly, lz, ux, uy, uz; // bounding box of the exact cell, relative to the seed
-    int flags;
-};
-
-__device__ __forceinline__ void t_bounds(const TSlab &S, int lane, TCell &c)
-{
-    float lx = INFINITY, ly = INFINITY, lz = INFINITY, ux = -INFINITY, uy = -INFINITY, uz = -INFINITY;
-    for (int j = 0; j < c.nv; ++j)
-    {
-        float4 X = S.vx[j][lane];
-        lx = fminf(lx, X.x - X.w);
-        ly = fminf(ly, X.y - X.w);
-        lz = fminf(lz, X.z - X.w);
-        ux = fmaxf(ux, X.x + X.w);
-        uy = fmaxf(uy, X.y + X.w);
-        uz = fmaxf(uz, X.z + X.w);
-    }
-    // the subtractions / additions above round: widen by a relative margin
-    c.lx = lx - 1e-6f * fabsf(lx);
-    c.ly = ly - 1e-6f * fabsf(ly);
-    c.lz = lz - 1e-6f * fabsf(lz);
-    c.ux = ux + 1e-6f * fabsf(ux);
-    c.uy = uy + 1e-6f * fabsf(uy);
-    c.uz = uz + 1e-6f * fabsf(uz);
-}
-
-// squared corner radius of the cell box over the octants allowed per axis
-__device__ __forceinline__ float t_axis_r2(float lo_rel, float hi_rel, float L, float U)
-{
-    float neg = fmaxf(-L, 0.0f), pos = fmaxf(U, 0.0f);
-    float a = lo_rel <= 0.0f ? neg * neg : 0.0f;
-    float b = hi_rel >= 0.0f ? pos * pos : 0.0f;
-    return fmaxf(a, b);
-}
-
-// Can a point of box [lo, hi] (absolute) with max weight mw remove a vertex?
-__device__ __forceinline__ bool t_box_may_clip(const TCell &c, float lx, float ly, float lz, float hx, float hy,
-                                               float hz, float mw)
-{
-    float rlx = lx - c.s.x, rly = ly - c.s.y, rlz = lz - c.s.z;
-    float rhx = hx - c.s.x, rhy = hy - c.s.y, rhz = hz - c.s.z;
-    float dx = fmaxf(rlx, 0.0f) + fmaxf(-rhx, 0.0f);
-    float dy = fmaxf(rly, 0.0f) + fmaxf(-rhy, 0.0f);
-    float dz = fmaxf(rlz, 0.0f) + fmaxf(-rhz, 0.0f);
-    float d2 = (dx * dx + dy * dy + dz * dz) * (1.0f - 1e-5f);
-    float r2 = (t_axis_r2(rlx, rhx, c.lx, c.ux) + t_axis_r2(rly, rhy, c.ly, c.uy) + t_axis_r2(rlz, rhz, c.lz, c.uz)) *
-               (1.0f + 1e-5f);
-    float dm = mw - c.s.w;
-    if (dm <= 0.0f)
-        return !(d2 > 4.0f * r2);
-    float num = d2 - dm * (1.0f + 1e-5f);
-    if (num <= 0.0f)
-        return true;
-    return !(num * num > 4.0f * d2 * r2);
-}
-
-// Can candidate q (plane n.x = h) remove a vertex? Directional corner test.
-__device__ __forceinline__ bool t_cand_may_clip(const TCell &c, const Cand &q)
-{
-    float ax = q.nx, ay = q.ny, az = q.nz;
-    float r2 = t_axis_r2(ax, ax, c.lx, c.ux) + t_axis_r2(ay, ay, c.ly, c.uy) + t_axis_r2(az, az, c.lz, c.uz);
-    float hm = q.h - q.eh; // lower bound of the exact h
-    if (hm <= 0.0f)
-        return true;
-    float n2 = q.nrm * q.nrm; // upper bound of |a|^2
-    return !(hm * hm > n2 * r2 * (1.0f + 1e-5f));
-}
-
-__device__ __forceinline__ void t_init(TSlab &S, int lane, TCell &c, const CellArgs &A)
-{
-    for (int code = 0; code < 6; ++code)
-    {
-        int ax = code >> 1, hi = code & 1;
-        float sc = ax == 0 ? c.s.x : (ax == 1 ? c.s.y : c.s.z);
-        float b = c.box[hi * 3 + ax];
-        float h = hi ? __fsub_rn(b, sc) : __fsub_rn(sc, b);
-        float sg = hi ? 1.0f : -1.0f;
-        S.pl[code][lane] = make_float4(ax == 0 ? sg : 0.0f, ax == 1 ? sg : 0.0f, ax == 2 ? sg : 0.0f, h);
-        S.pe[code][lane] = kEps * fabsf(h);
-        S.pid[code][lane] = -1 - code;
-    }
-    for (int k = 0; k < 8; ++k)
-    {
-        int sx = k & 1, sy = (k >> 1) & 1, sz = (k >> 2) & 1;
-        int px = sx, py = 2 + sy, pz = 4 + sz;
-        int sign = (sx ? 1 : -1) * (sy ? 1 : -1) * (sz ? 1 : -1);
-        int p0 = sign > 0 ? px : py, p1 = sign > 0 ? py : px, p2 = pz;
-        float vr;
-        S.vx[k][lane] =
-            make_vertex(S.pl[p0][lane], S.pe[p0][lane], S.pl[p1][lane], S.pe[p1][lane], S.pl[p2][lane], S.pe[p2][lane], vr);
-        S.vt[k][lane] = (unsigned)p0 | ((unsigned)p1 << 8) | ((unsigned)p2 << 16);
-    }
-    c.nv = 8;
-    c.np = 6;
-    c.flags = 0;
-    t_bounds(S, lane, c);
-}
-
-// drop planes no vertex references (vertices keep their slots)
-__device__ __noinline__ int t_gc(TSlab &S, int lane, int nv, int np)
-{
-    unsigned long long live = 0;
-    for (int j = 0; j < nv; ++j)
-    {
-        unsigned t = S.vt[j][lane];
-        live |= (1ull << (t & 255u)) | (1ull << ((t >> 8) & 255u)) | (1ull << ((t >> 16) & 255u));
-    }
-    int w = 0;
-    for (int p = 0; p < np; ++p)
-        if ((live >> p) & 1ull)
-        {
-            if (w != p)
-            {
-                S.pl[w][lane] = S.pl[p][lane];
-                S.pe[w][lane] = S.pe[p][lane];
-                S.pid[w][lane] = S.pid[p][lane];
-            }
-            ++w;
-        }
-    for (int j = 0; j < nv; ++j)
-    {
-        unsigned t = S.vt[j][lane], out = 0;
-        for (int e = 0; e < 3; ++e)
-        {
-            unsigned p = (t >> (8 * e)) & 255u;
-            unsigned q = __popcll(live & ((1ull << p) - 1ull));
-            out |= q << (8 * e);
-        }
-        S.vt[j][lane] = out;
-    }
-    return w;
-}
-
-__device__ __forceinline__ bool tri_has_edge(unsigned u, unsigned a, unsigned b)
-{
-    unsigned u0 = u & 255u, u1 = (u >> 8) & 255u, u2 = (u >> 16) & 255u;
-    return (u0 == a && u1 == b) || (u1 == a && u2 == b) || (u2 == a && u0 == b);
-}
-
-__device__ __forceinline__ int t_clip(TSlab &S, int lane, TCell &c, const Cand &q, const CellArgs &A,
-                                      unsigned &n_fp64, unsigned &n_exp)
-{
-    unsigned long long rm = 0;
-    for (int j = 0; j < c.nv; ++j)
-    {
-        int r = side_fp32(S.vx[j][lane], q);
-        if (r < 0)
-        {
-            unsigned t = S.vt[j][lane];
-            int used = 0;
-            r = side_exact(S.pid[t & 255u][lane], S.pid[(t >> 8) & 255u][lane], S.pid[(t >> 16) & 255u][lane], q.id,
-                           A.pts, A.oid, c.box, c.s, c.soid, &used);
-            ++n_fp64;
-            n_exp += used;
-            if (r < 0)
-            {
-                c.flags |= kFlagError;
-                r = 0;
-            }
-        }
-        if (r)
-            rm |= 1ull << j;
-    }
-    if (!rm)
-        return kClipNone;
-    int R = __popcll(rm);
-    if (R == c.nv)
-    {
-        c.flags |= kFlagEmpty;
-        c.nv = 0;
-        return kClipEmptied;
-    }
-    if (c.np >= kTCap)
-    {
-        c.np = t_gc(S, lane, c.nv, c.np);
-        if (c.np >= kTCap)
-            return kClipDefer;
-    }
-    int P = c.np++;
-    S.pl[P][lane] = make_float4(q.nx, q.ny, q.nz, q.h);
-    S.pe[P][lane] = q.eh;
-    S.pid[P][lane] = q.id;
-    // boundary edges of the removed region
-    unsigned short be[kTMaxBoundary];
-    int nb = 0;
-    for (unsigned long long m1 = rm; m1; m1 &= m1 - 1ull)
-    {
-        int j = __ffsll((long long)m1) - 1;
-        unsigned t = S.vt[j][lane];
-        unsigned tv[3] = {t & 255u, (t >> 8) & 255u, (t >> 16) & 255u};
-        for (int e = 0; e < 3; ++e)
-        {
-            unsigned x = tv[e], y = tv[(e + 1) % 3];
-            bool interior = false;
-            for (unsigned long long m2 = rm; m2 && !interior; m2 &= m2 - 1ull)
-            {
-                int k = __ffsll((long long)m2) - 1;
-                interior = k != j && tri_has_edge(S.vt[k][lane], y, x);
-            }
-            if (!interior)
-            {
-                if (nb >= kTMaxBoundary)
-                    return kClipDefer;
-                be[nb++] = (unsigned short)(x | (y << 8));
-            }
-        }
-    }
-    int keepn = c.nv - R;
-    if (keepn + nb > kTCap)
-        return kClipDefer;
-    // compact: kept vertices at or above keepn move into the holes below keepn
-    unsigned long long low = keepn >= 64 ? ~0ull : ((1ull << keepn) - 1ull);
-    unsigned long long all = c.nv >= 64 ? ~0ull : ((1ull << c.nv) - 1ull);
-    unsigned long long holes = rm & low;
-    unsigned long long src = (all & ~rm) & ~low;
-    while (holes)
-    {
-        int j = __ffsll((long long)holes) - 1, k = __ffsll((long long)src) - 1;
-        holes &= holes - 1ull;
-        src &= src - 1ull;
-        S.vx[j][lane] = S.vx[k][lane];
-        S.vt[j][lane] = S.vt[k][lane];
-    }
-    float4 pP = S.pl[P][lane];
-    float eP = S.pe[P][lane];
-    for (int b = 0; b < nb; ++b)
-    {
-        unsigned x = be[b] & 255u, y = be[b] >> 8;
-        float vr;
-        S.vx[keepn + b][lane] = make_vertex(pP, eP, S.pl[x][lane], S.pe[x][lane], S.pl[y][lane], S.pe[y][lane], vr);
-        S.vt[keepn + b][lane] = (unsigned)P | (x << 8) | (y << 16);
-    }
-    c.nv = keepn + nb;
-    return kClipChanged;
-}
-
-struct TStats
-{
-    unsigned tests, fp64, exp, nodes, leaves, clips, cands;
-};
-
-// returns false when the cell finished early (empty / deferred)
-__device__ __forceinline__ bool t_try(TSlab &S, int lane, TCell &c, int j, const CellArgs &A, TStats &ts, bool &changed)
-{
-    float4 p = A.pts[j];
-    if (p.x == c.s.x && p.y == c.s.y && p.z == c.s.z)
-        return true; // coincident points never clip each other
-    Cand q = make_cand(c.s, p, j);
-    if (!t_cand_may_clip(c, q))
-        return true;
-    ++ts.cands;
-    ts.tests += c.nv;
-    int r = t_clip(S, lane, c, q, A, ts.fp64, ts.exp);
-    if (r == kClipEmptied)
-        return false;
-    if (r == kClipDefer)
-    {
-        c.flags |= kFlagDefer;
-        return false;
-    }
-    if (r == kClipChanged)
-    {
-        ++ts.clips;
-        changed = true;
-    }
-    return true;
-}
-
-__device__ __forceinline__ void t_process(TSlab &S, int lane, TCell &c, const CellArgs &A, TStats &ts)
-{
-    t_init(S, lane, c, A);
-    const int n = A.n, i = c.si;
-    const bool guessing = A.guesses != nullptr;
-    bool changed = false;
-    if (guessing)
-    {
-        int g0 = A.guess_off[c.soid], g1 = A.guess_off[c.soid + 1];
-        for (int g = g0; g < g1; ++g)
-        {
-            int o = A.guesses[g];
-            if (o < 0 || o >= n)
-                continue;
-            int j = A.rank[o];
-            if (j == i)
-                continue;
-            bool dup = false;
-            for (int t = 0; t < c.np && !dup; ++t)
-                dup = S.pid[t][lane] == j;
-            if (dup)
-                continue;
-            if (!t_try(S, lane, c, j, A, ts, changed))
-                return;
-        }
-    }
-    else
-    {
-        for (int d = 1; d <= A.window; ++d)
-        {
-            if (i - d >= 0 && !t_try(S, lane, c, i - d, A, ts, changed))
-                return;
-            if (i + d < n && !t_try(S, lane, c, i + d, A, ts, changed))
-                return;
-        }
-    }
-    if (changed)
-        t_bounds(S, lane, c);
-    int stk[kTStack];
-    int sp = 0;
-    stk[sp++] = c.root;
-    while (sp > 0)
-    {
-        int ref = stk[--sp];
-        if (ref_is_leaf(ref))
-        {
-            ++ts.leaves;
-            int first = leaf_first(ref), count = leaf_count(ref);
-            changed = false;
-            for (int l = 0; l < count; ++l)
-            {
-                int j = first + l;
-                if (j == i)
-                    continue;
-                if (!guessing && j >= i - A.window && j <= i + A.window)
-                    continue;
-                if (guessing)
-                {
-                    bool dup = false;
-                    for (int t = 0; t < c.np && !dup; ++t)
-                        dup = S.pid[t][lane] == j;
-                    if (dup)
-                        continue;
-                }
-                if (!t_try(S, lane, c, j, A, ts, changed))
-                    return;
-            }
-            if (changed)
-                t_bounds(S, lane, c);
-            continue;
-        }
-        ++ts.nodes;
-        const float4 *r = A.rec + 4 * (size_t)ref;
-        float4 r0 = __ldg(r), r1 = __ldg(r + 1), r2 = __ldg(r + 2), r3 = __ldg(r + 3);
-        bool c0 = t_box_may_clip(c, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r3.z);
-        bool c1 = t_box_may_clip(c, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.w);
-        if (sp + 2 > kTStack)
-        {
-            c.flags |= kFlagDefer;
-            return;
-        }
-        int ref0 = __float_as_int(r3.x), ref1 = __float_as_int(r3.y);
-        if (c0 && c1)
-        {
-            // nearer child (by box distance from the seed) on top
-            float d0 = fmaxf(fmaxf(r0.x - c.s.x, c.s.x - r0.w), 0.0f) + fmaxf(fmaxf(r0.y - c.s.y, c.s.y - r1.x), 0.0f) +
-                       fmaxf(fmaxf(r0.z - c.s.z, c.s.z - r1.y), 0.0f);
-            float d1 = fmaxf(fmaxf(r1.z - c.s.x, c.s.x - r2.y), 0.0f) + fmaxf(fmaxf(r1.w - c.s.y, c.s.y - r2.z), 0.0f) +
-                       fmaxf(fmaxf(r2.x - c.s.z, c.s.z - r2.w), 0.0f);
-            stk[sp++] = d0 <= d1 ? ref1 : ref0;
-            stk[sp++] = d0 <= d1 ? ref0 : ref1;
-        }
-        else if (c0)
-            stk[sp++] = ref0;
-        else if (c1)
-            stk[sp++] = ref1;
-    }
-}
-
-__device__ __forceinline__ bool t_write(const TSlab &S, int lane, const TCell &c, const CellArgs &A)
-{
-    int oi = c.soid;
-    if (c.flags & kFlagEmpty)
-    {
-        A.deg[oi] = 0;
-        A.status[oi] = kEmptyCell;
-        return true;
-    }
-    unsigned long long live = 0;
-    for (int j = 0; j < c.nv; ++j)
-    {
-        unsigned t = S.vt[j][lane];
-        live |= (1ull << (t & 255u)) | (1ull << ((t >> 8) & 255u)) | (1ull << ((t >> 16) & 255u));
-    }
-    // box planes have no neighbour (after plane GC they can sit in any slot)
-    for (unsigned long long m = live; m; m &= m - 1ull)
-    {
-        int p = __ffsll((long long)m) - 1;
-        if (S.pid[p][lane] < 0)
-            live &= ~(1ull << p);
-    }
-    int cnt = __popcll(live);
-    if (cnt > kRowWidth)
-        return false;
-    int *row = A.rows + (size_t)oi * kRowWidth;
-    int k = 0;
-    for (unsigned long long m = live; m; m &= m - 1ull)
-    {
-        int p = __ffsll((long long)m) - 1;
-        int o = A.oid[S.pid[p][lane]];
-        // insertion into the sorted prefix row[0..k)
-        int t = k;
-        while (t > 0 && row[t - 1] > o)
-        {
-            row[t] = row[t - 1];
-            --t;
-        }
-        row[t] = o;
-        ++k;
-    }
-    A.deg[oi] = cnt;
-    A.status[oi] = c.nv > kMaxVertsRef ? kVertexOverflow : kSuccess;
-    return true;
-}
-
-__global__ void __launch_bounds__(256, 4) k_tcells(CellArgs A, TSlab *slabs)
-{
-    int lane = threadIdx.x & 31;
-    size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    TSlab &S = slabs[gw];
-    TStats ts = {0, 0, 0, 0, 0, 0, 0};
-    int64_t count = A.end - A.begin;
-    for (;;)
-    {
-        int base = 0;
-        if (lane == 0)
-            base = atomicAdd(&A.counters[0], 32);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= count)
-            break;
-        int t = base + lane;
-        if (t < count)
-        {
-            TCell c;
-            c.si = (int)(A.begin + t);
-            c.s = A.pts[c.si];
-            c.soid = A.oid[c.si];
-            {
-                int cc = cloud_of(A.cloud_off, A.num_clouds, c.si);
-                c.box = A.box + 8 * cc;
-                c.root = A.cloud_root[cc];
-            }
-            t_process(S, lane, c, A, ts);
-            if (c.flags & kFlagError)
-                atomicExch(&A.counters[2], 1);
-            bool done = !(c.flags & kFlagDefer) && t_write(S, lane, c, A);
-            if (!done)
-            {
-                A.deg[c.soid] = 0;
-                A.status[c.soid] = kPlaneOverflow;
-                int d = atomicAdd(&A.counters[1], 1);
-                A.big_list[d] = c.si;
-                atomicAdd(&A.stats[kStatDeferred], 1ull);
-            }
-        }
-        __syncwarp();
-    }
-    unsigned v[7] = {ts.tests, ts.fp64, ts.exp, ts.nodes, ts.leaves, ts.clips, ts.cands};
-    const int idx[7] = {kStatTests, kStatFp64, kStatExpansion, kStatNodes, kStatLeaves, kStatClips, kStatCandidates};
-#pragma unroll
-    for (int k = 0; k < 7; ++k)
-    {
-        unsigned long long sum = v[k];
-        for (int o = 16; o > 0; o >>= 1)
-            sum += __shfl_down_sync(kFull, sum, o);
-        if (lane == 0 && sum)
-            atomicAdd(&A.stats[idx[k]], sum);
-    }
-}
-
-int tcell_threads() { return 148 * 1024; }
-size_t tcell_slab_bytes() { return sizeof(TSlab) * (size_t)(tcell_threads() / 32); }
 
 int big_warps() { return 148 * kMaxWarpsPerSM; } // one slab per resident warp
 size_t huge_slab_bytes() { return sizeof(CellMem<kCapHuge, kStackHuge>) * (size_t)kHugeSlabs; }
@@ -2192,7 +1638,6 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.big_cap = 0;
     A.slabs = (char *)ws.big_slabs;
     A.huge_slabs = (char *)ws.huge_slabs;
-    A.inline_big = 0;
     A.radius_out = cl.radius_out;
     A.work_out = reinterpret_cast<int4 *>(cl.work_out);
     A.geometry_out = reinterpret_cast<float4 *>(cl.geometry_out);
@@ -2209,21 +1654,6 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
     A.status = status;
     cudaMemsetAsync(ws.counters, 0, sizeof(int), st); // work counter
     int64_t cells = cl.cell_end - cl.cell_begin;
-    if (cl.min_blocks == 0)
-    {
-        // thread per cell: persistent grid, at most one slab per resident warp
-        int bps = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_tcells, 256, 0);
-        if (bps < 1)
-            bps = 1;
-        int64_t grid = std::min<int64_t>((int64_t)num_sms * bps, tcell_threads() / 256);
-        grid = std::min<int64_t>(grid, (cells + 255) / 256);
-        if (grid < 1)
-            grid = 1;
-        ++g_launches;
-        k_tcells<<<(unsigned)grid, 256, 0, st>>>(A, (TSlab *)ws.tslabs);
-        return;
-    }
     // variants: register budget (2 or 3 blocks per SM), initial guesses, search radius per cell
     // (a search radius is not used together with initial guesses)
     void (*kern)(CellArgs);
@@ -2237,7 +1667,6 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerBlock * 32, 0);
     if (blocks_per_sm < 1)
         blocks_per_sm = 1;
-    A.inline_big = cl.inline_big;
     A.big_cap = cl.big_cap;
     int64_t grid = std::min<int64_t>((int64_t)num_sms * blocks_per_sm, big_warps() / kWarpsPerBlock);
     int64_t need = (cells + kWarpsPerBlock - 1) / kWarpsPerBlock;

@@ -141,7 +141,6 @@ struct Workspace
     int *big_rows;        // [big_cap * kBigRowWidth]
     void *big_slabs;      // per-warp state of the large-capacity pass
     void *huge_slabs;     // [kHugeSlabs] state of cells that outgrew the large capacity
-    void *tslabs;         // per-warp state of the thread-per-cell pass
     // CSR
     int *cnt;             // [N] kept directed entries per row
     int *miss;            // [N] reverse entries to add per row
@@ -153,8 +152,6 @@ struct Workspace
 int big_warps();   // number of warps of the large-capacity pass
 size_t big_slab_bytes();
 size_t huge_slab_bytes();
-int tcell_threads(); // resident threads of the thread-per-cell pass
-size_t tcell_slab_bytes();
 size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws);
 
 } // namespace pg

@@ -33,14 +33,13 @@ struct CellLaunch
     const int *guess_off;     // [N+1] offsets of the initial guesses
     int64_t cell_begin, cell_end; // sorted-slot range of this launch
     int weighted;
-    int min_blocks; // register-budget variant of the cell kernel (2, 3 or 4 blocks per SM)
+    int min_blocks; // register-budget variant of the cell kernel (2 or 3 blocks per SM)
     int64_t big_cap; // deferred-row slots
     float *radius_out; // per original id: certified radius of the final cell, or nullptr
     int *work_out;     // per original id: nodes, leaves, candidates, peak queue; or nullptr
     float *geometry_out; // per original id: centroid x, y, z and volume of the cell; or nullptr
     int use_hint;      // the workspace holds a search radius per sorted slot
     int fp32_only;     // side tests in FP32 only (no escalation; not exact)
-    int inline_big;    // rebuild cells that outgrow 64 slots in the same warp at once (else a second launch)
 };
 void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int num_sms, cudaStream_t st);
 void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st);

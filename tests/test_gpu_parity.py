@@ -159,15 +159,6 @@ def test_initial_guesses_do_not_change_results(dev, oracle):
         _assert_same((g.adjacency.cpu().numpy(), g.offsets.cpu().numpy(), g.status.cpu().numpy()), exp, "guesses")
 
 
-def test_thread_per_cell_variant(dev, oracle, monkeypatch):
-    """The thread-per-cell kernel (PG_CELL_MIN_BLOCKS=0) gives the same diagram."""
-    from paragram_b200 import workloads as W
-
-    monkeypatch.setenv("PG_CELL_MIN_BLOCKS", "0")
-    pts, w = W.power_uniform(20_000, seed=21)
-    _assert_same(_gpu(dev, pts, w), oracle.diagram(pts, w), "thread-per-cell")
-
-
 def test_full_size_properties(dev):
     """5M clustered Voronoi: symmetric, sorted, no self loops, consistent offsets."""
     from paragram_b200 import workloads as W

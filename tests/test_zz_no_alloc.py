@@ -62,3 +62,20 @@ def test_noalloc_empty(dev):
     assert lib.pg_degrees_to_offsets_noalloc(0, None, out.data_ptr(), None) == 0
     torch.cuda.synchronize(dev)
     assert out.item() == 0
+
+
+def test_noalloc_three_level_scan(dev):
+    """More than 2048^2 rows: the scan recurses three levels inside the static scratch. Two
+    calls in a row, each against torch's cumulative sum."""
+    from paragram_b200 import _lib
+
+    lib = _lib.load()
+    g = torch.Generator(device=dev).manual_seed(5)
+    for n in (5_000_001, 4_194_305):
+        degrees = torch.randint(0, 40, (n,), device=dev, dtype=torch.int32, generator=g)
+        exp = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+        exp[1:] = torch.cumsum(degrees.to(torch.int64), 0)
+        out = torch.full((n + 1,), -7, dtype=torch.int32, device=dev)
+        assert _noalloc(lib, degrees, out) == 0, _lib.last_error(lib)
+        torch.cuda.synchronize(dev)
+        assert torch.equal(out.to(torch.int64), exp)
