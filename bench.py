@@ -20,10 +20,13 @@ lattice, power), surface_batch_256 (256 surface clouds in one CUDA-graph batch).
 For N > 1 (torch.distributed.run, one process per GPU) every rank builds its
 own diagram of an equally sized, differently seeded point set (weak scaling;
 cells shard without any data exchange) and the step time is the max over
-ranks. ``--impl reference`` times the CPU restatement of the reference's
-construction (the parity oracle, all host threads) on a bounded sample of the
-same workload; the reference's CUDA extension cannot be built (its cuBQL
-dependency is not vendored).
+ranks. ``--impl reference`` times the reference's own CUDA extension
+(``oracle/_ref``: its unmodified sources compiled with a project-written
+stand-in for its absent cuBQL dependency) on the same workload, counting its
+construction phase (cells + CSR) by its own timers; without that build or a
+GPU (or with ``--reference-cpu``) it times the CPU restatement of the
+reference's construction (the parity oracle, all host threads) on a bounded
+sample of the workload.
 """
 
 from __future__ import annotations
@@ -214,9 +217,86 @@ def cpu_oracle_rate_clouds(clouds, sample: int) -> dict:
             "cells_s": secs - tree, "wall_s": time.perf_counter() - t0, "clouds": used}
 
 
+def run_reference_cuda(args, spec, world) -> bool:
+    """The reference's own CUDA extension (oracle/_ref: its unmodified sources compiled with a
+    project-written stand-in for its absent cuBQL dependency) on the same workload.
+
+    A step is one reference call (paragram.voronoi_diagram / power_diagram's pybind function). Its
+    value is cells / the reference's own "Construction time" (printed with debug=True: the cell
+    kernel, the CSR gather, symmetrisation and cumsum, voronoi_ultra.cu:368-373), which leaves out
+    its BVH build and kNN: the stand-in builds the BVH on the host, which would not be a fair
+    stand-in for cuBQL's GPU builder. The full call's wall time is reported beside it.
+    Returns False when the extension or a GPU is missing.
+    """
+    import torch
+
+    from oracle import pg_ref
+
+    if not (pg_ref.available() and torch.cuda.is_available()):
+        return False
+    dev = torch.device("cuda:0")
+    pts, w = make_points(spec, seed=0)
+    if spec["kind"] == "surfaces":
+        # the reference has no batch API: one call per cloud, the clouds in order up to ~2M points
+        take, tot = [], 0
+        for c in pts:
+            if tot >= 2_000_000:
+                break
+            take.append(torch.from_numpy(c).to(dev))
+            tot += len(c)
+        calls = [(lambda t=t, **kw: pg_ref.voronoi(t, **kw)) for t in take]
+        sample = f"the first {len(take)} of {len(pts)} clouds ({tot} points), one reference call per cloud"
+    else:
+        t = torch.from_numpy(pts).to(dev)
+        tw = None if w is None else torch.from_numpy(w).to(dev)
+        calls = [(lambda **kw: pg_ref.voronoi(t, **kw))] if tw is None else [(lambda **kw: pg_ref.power(t, tw, **kw))]
+        tot = len(pts)
+        sample = f"the whole {tot}-point workload per step"
+    big = tot > 10_000_000  # the stand-in's host BVH build takes tens of seconds per call
+    warm, steps = (min(args.warmup, 1), min(args.steps, 2)) if big else (args.warmup, args.steps)
+
+    def one_step():
+        cons, wall = 0.0, 0.0
+        for fn in calls:
+            t0 = time.perf_counter()
+            ph = pg_ref.phase_ms(fn) or {}
+            wall += time.perf_counter() - t0
+            cons += sum(v for k, v in ph.items() if k.endswith("Construction"))
+        return cons, wall
+
+    for _ in range(warm):
+        one_step()
+    cons, walls = [], []
+    for _ in range(steps):
+        c, wl = one_step()
+        cons.append(c)
+        walls.append(wl)
+    ms = statistics.median(cons)
+    value = tot / (ms / 1e3) / 1e6
+    line = {
+        "impl": "reference", "metric": "Mcells/s", "value": value, "unit": "Mcells/s", "n_gpus": world,
+        "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "n_points": tot, "weighted": spec["weighted"]},
+        "cpu_baseline": {"value": value, "unit": "Mcells/s", "cores": 1, "kind": "reference",
+                         "sample": sample + "; the reference's CUDA extension on the GPU, its construction phase "
+                                   "(cells + CSR) timed by its own debug timers; the BVH comes from the "
+                                   "stand-in's single-threaded host builder and is not counted"},
+        "e2e": {"value": value, "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_full_call": {"ms_per_step": 1e3 * statistics.median(walls),
+                                "note": "wall time of the whole call, including the stand-in's host BVH build"},
+        "note": "the reference's own kernels (oracle/_ref); cuBQL replaced by a project-written stand-in",
+    }
+    print(json.dumps(line), flush=True)
+    return True
+
+
 def run_reference(args, spec, rank, world):
-    """CPU restatement of the reference's construction on the host cores (rank 0 only)."""
+    """The reference on the same workload (rank 0 only): its CUDA extension where it is built and a
+    GPU is present, else the CPU restatement of its construction on the host cores."""
     if rank != 0:
+        return
+    if not args.reference_cpu and run_reference_cuda(args, spec, world):
         return
     pts, w = make_points(spec, seed=0)
     sample = args.cpu_sample
@@ -252,7 +332,7 @@ def run_reference(args, spec, rank, world):
                                    f"kd-tree over all points ({info['tree_s']:.2f} s) + sampled cells "
                                    f"({info['cells_s']:.2f} s), extrapolated to all cells"},
         "e2e": {"value": value, "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "reference CUDA extension not buildable (cuBQL submodule absent); CPU oracle port timed",
+        "note": "CPU restatement of the reference's construction (the oracle port) timed on the host",
     }
     print(json.dumps(line), flush=True)
 
@@ -573,6 +653,9 @@ def main():
     ap.add_argument("--workload", default="clustered_voronoi_5m", choices=sorted(WORKLOADS))
     ap.add_argument("--cpu-sample", type=int, default=200_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--reference-cpu", action="store_true",
+                    help="with --impl reference: time the CPU restatement even where the reference's CUDA "
+                         "extension is built")
     ap.add_argument("--plain", action="store_true", help="time the plain build only (no learned radius)")
     ap.add_argument("--fp32-only-too", action="store_true",
                     help="also time the build with FP32-only side tests (no FP64 / exact escalation)")

@@ -86,6 +86,20 @@ typedef struct pg_options
                               centroid (x, y, z) and the volume of its cell (the geometry the reference
                               computes and discards, voronoi_ultra.cu:125-138). An empty cell gives
                               volume 0 and a NaN centroid; a plane_overflow cell NaN. */
+    /* Vertex export (no reference counterpart; the reference keeps its vertices in per-thread
+     * scratch and discards them, voronoi_ultra.cu:125-138). Added in version 200: a caller must
+     * check pg_version() >= 200 before passing a pg_options with these fields, since an older
+     * library reads the shorter struct. */
+    int32_t vertex_cap;    /* vertices per cell that vertices_out / vertex_planes_out hold (0: none) */
+    float *vertices_out;   /* device float32 [num_points * vertex_cap * 4], 16-byte aligned, or NULL: per
+                              cell, its vertices relative to the cell's point (x, y, z) and w, a
+                              rigorous bound on the distance from (x, y, z) to the exact vertex (the
+                              error radius of the FP32 side tests) */
+    int32_t *vertex_planes_out; /* device int32 [num_points * vertex_cap * 3] or NULL: the three planes
+                              meeting at each vertex: the neighbour's point index for a bisector, or
+                              -1 - code for a face of the box (code = 2 * axis + 1 on the high side) */
+    int32_t *vertex_count_out; /* device int32 [num_points] or NULL: the number of vertices of each cell
+                              (0 for an empty cell); vertices beyond vertex_cap are counted, not written */
 } pg_options;
 
 /* Learned search radius (no reference counterpart). A 16 -> 64 -> 64 -> 2 MLP

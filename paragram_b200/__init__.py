@@ -8,12 +8,13 @@ fallback -- calling the API without the built library raises ImportError.
 
 from ._api import Diagram, power_diagram, voronoi_diagram
 from .batch import build_batch
-from .geometry import cell_geometry
+from .geometry import cell_geometry, cell_vertices
 
 __all__ = [
     "Diagram",
     "build_batch",
     "cell_geometry",
+    "cell_vertices",
     "power_diagram",
     "voronoi_diagram",
 ]

@@ -30,6 +30,10 @@ class PgOptions(ctypes.Structure):
         ("features_out", ctypes.c_void_p),
         ("order_out", ctypes.c_void_p),
         ("geometry_out", ctypes.c_void_p),
+        ("vertex_cap", ctypes.c_int32),
+        ("vertices_out", ctypes.c_void_p),
+        ("vertex_planes_out", ctypes.c_void_p),
+        ("vertex_count_out", ctypes.c_void_p),
     ]
 
 

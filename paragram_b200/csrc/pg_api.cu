@@ -73,6 +73,7 @@ size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
     w.flags = (int *)take(4 * N);
     w.nbox = (float4 *)take(32 * N);
     w.records = (float4 *)take(64 * N);
+    w.region = (float4 *)take(32 * N);
     w.rparent = (int *)take(4 * N);
     w.pleaf = (int *)take(4 * N);
     w.hint = (float *)take(4 * N);
@@ -85,6 +86,7 @@ size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
     w.cnt = (int *)take(4 * N);
     w.miss = (int *)take(4 * N);
     w.fill = (int *)take(4 * N);
+    w.rmask = (unsigned long long *)take(16 * N);
     w.sizes = (uint32_t *)take(4 * (N + 1));
     // per-cloud segments last, so that every other offset is independent of the cloud count
     w.bounds = (int *)take(8 * C * sizeof(int));
@@ -158,7 +160,8 @@ __global__ void k_hint_gather(int64_t n, const int *oid, const float *radius, fl
 static int check_counters(const int *host, int64_t n)
 {
     if (host[2] == 1)
-        return fail(PG_ERR_INTERNAL, "exact predicate exceeded its expansion capacity");
+        return fail(PG_ERR_INTERNAL, "cell kernel consistency check failed (exact predicate capacity or "
+                                     "polytope topology)");
     if (host[2] == 2)
         return fail(PG_ERR_INTERNAL, "a cloud's points do not form one BVH subtree");
     if (host[1] > big_cap(n))
@@ -177,7 +180,9 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
 {
     g_last_error.clear();
     cudaStream_t st = (cudaStream_t)stream;
-    pg_options opt = {8, -1, 0, 0, 0, 0, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    pg_options opt{};
+    opt.knn = 8;
+    opt.leaf_size = -1;
     if (options)
         opt = *options;
     const bool sync = num_edges != nullptr;
@@ -201,6 +206,10 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         return fail(PG_ERR_INVALID, "work_out must be 16-byte and radius_out 4-byte aligned");
     if (((uintptr_t)opt.geometry_out & 15u) != 0)
         return fail(PG_ERR_INVALID, "geometry_out must be 16-byte aligned");
+    if (opt.vertex_cap < 0 || ((opt.vertices_out || opt.vertex_planes_out) && opt.vertex_cap == 0))
+        return fail(PG_ERR_INVALID, "vertex_cap must be >= 0, and > 0 when vertices_out or vertex_planes_out is set");
+    if (((uintptr_t)opt.vertices_out & 15u) != 0)
+        return fail(PG_ERR_INVALID, "vertices_out must be 16-byte aligned");
     size_t need = workspace_layout(n, num_clouds, nullptr, nullptr);
     if (workspace_bytes < need)
         return fail(PG_ERR_INVALID, "workspace too small: need " + std::to_string(need) + " bytes");
@@ -258,6 +267,10 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     cl.radius_out = opt.radius_out;
     cl.work_out = opt.work_out;
     cl.geometry_out = opt.geometry_out;
+    cl.vertex_cap = opt.vertex_cap;
+    cl.vertices_out = opt.vertices_out;
+    cl.vertex_planes_out = opt.vertex_planes_out;
+    cl.vertex_count_out = opt.vertex_count_out;
     cl.use_hint = 0;
     if (opt.features_out != nullptr)
         features_launch(ws, n, num_clouds, opt.features_out, st);
@@ -349,7 +362,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
 
 extern "C" {
 
-int pg_version(void) { return 102; }
+int pg_version(void) { return 200; }
 
 const char *pg_last_error(void) { return pg::g_last_error.c_str(); }
 

@@ -42,15 +42,24 @@ __device__ __forceinline__ bool row_has(const int *r, int d, int x)
     return false;
 }
 
+// Rows are visited in curve order (thread t takes sorted slot t), so that a
+// block's cells are spatial neighbours and the rows their searches read are
+// shared through L2. Per row, two bit masks over its directed entries record
+// what the fill needs: entry k is kept (its target has a nonempty row) and
+// entry k's target does not list this row (a reverse entry to add). Rows of
+// deferred cells (up to kBigRowWidth entries) do not fit the masks and are
+// re-examined by the fill.
 __global__ void k_csr_count(const int *__restrict__ rows, const int *__restrict__ big_rows,
-                            const int *__restrict__ deg, int64_t n, int *__restrict__ cnt, int *__restrict__ miss)
+                            const int *__restrict__ deg, const int *__restrict__ oid, int64_t n, int *__restrict__ cnt,
+                            int *__restrict__ miss, unsigned long long *__restrict__ masks)
 {
-    int64_t uu = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (uu >= n)
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n)
         return;
-    int u = (int)uu, d;
+    int u = oid[t], d;
     const int *r = row_of(rows, big_rows, deg, u, d);
     int kept = 0;
+    unsigned long long keep_bits = 0, miss_bits = 0;
     for (int k = 0; k < d; ++k)
     {
         int v = r[k], dv;
@@ -58,10 +67,18 @@ __global__ void k_csr_count(const int *__restrict__ rows, const int *__restrict_
         if (dv <= 0)
             continue;
         ++kept;
-        if (!row_has(rv, dv, u))
+        bool missing = !row_has(rv, dv, u);
+        if (missing)
             atomicAdd(&miss[v], 1);
+        if (k < 64)
+        {
+            keep_bits |= 1ull << k;
+            miss_bits |= (unsigned long long)missing << k;
+        }
     }
     cnt[u] = kept;
+    masks[2 * (size_t)u] = keep_bits;
+    masks[2 * (size_t)u + 1] = miss_bits;
 }
 
 __global__ void k_csr_sizes(const int *__restrict__ cnt, const int *__restrict__ miss, int64_t n,
@@ -73,15 +90,31 @@ __global__ void k_csr_sizes(const int *__restrict__ cnt, const int *__restrict__
 }
 
 __global__ void k_csr_fill(const int *__restrict__ rows, const int *__restrict__ big_rows, const int *__restrict__ deg,
-                           int64_t n, const int *__restrict__ off, const int *__restrict__ cnt, int *__restrict__ fill,
-                           int *__restrict__ adj)
+                           const int *__restrict__ oid, int64_t n, const int *__restrict__ off,
+                           const int *__restrict__ cnt, const unsigned long long *__restrict__ masks,
+                           int *__restrict__ fill, int *__restrict__ adj)
 {
-    int64_t uu = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (uu >= n)
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n)
         return;
-    int u = (int)uu, d;
+    int u = oid[t], d;
     const int *r = row_of(rows, big_rows, deg, u, d);
     int pos = off[u];
+    if (d <= 64)
+    {
+        // the count pass already decided every entry
+        unsigned long long keep_bits = masks[2 * (size_t)u], miss_bits = masks[2 * (size_t)u + 1];
+        for (int k = 0; k < d; ++k)
+        {
+            if (!((keep_bits >> k) & 1ull))
+                continue;
+            int v = r[k];
+            adj[pos++] = v;
+            if ((miss_bits >> k) & 1ull)
+                adj[off[v] + cnt[v] + atomicAdd(&fill[v], 1)] = u;
+        }
+        return;
+    }
     for (int k = 0; k < d; ++k)
     {
         int v = r[k], dv;
@@ -117,7 +150,7 @@ void csr_count(const Workspace &ws, int64_t n, int32_t *offsets, cudaStream_t st
     unsigned g = (unsigned)((n + 255) / 256);
     cudaMemsetAsync(ws.miss, 0, sizeof(int) * (size_t)n, st);
     ++g_launches;
-    k_csr_count<<<g, 256, 0, st>>>(ws.rows, ws.big_rows, ws.deg, n, ws.cnt, ws.miss);
+    k_csr_count<<<g, 256, 0, st>>>(ws.rows, ws.big_rows, ws.deg, ws.oid, n, ws.cnt, ws.miss, ws.rmask);
     ++g_launches;
     k_csr_sizes<<<g, 256, 0, st>>>(ws.cnt, ws.miss, n, ws.sizes);
     exclusive_scan(ws.sizes, (uint32_t *)offsets, n, ws.scan_tmp, st);
@@ -128,7 +161,8 @@ void csr_fill(const Workspace &ws, int64_t n, const int32_t *offsets, int32_t *a
     unsigned g = (unsigned)((n + 255) / 256);
     cudaMemsetAsync(ws.fill, 0, sizeof(int) * (size_t)n, st);
     ++g_launches;
-    k_csr_fill<<<g, 256, 0, st>>>(ws.rows, ws.big_rows, ws.deg, n, offsets, ws.cnt, ws.fill, adjacency);
+    k_csr_fill<<<g, 256, 0, st>>>(ws.rows, ws.big_rows, ws.deg, ws.oid, n, offsets, ws.cnt, ws.rmask, ws.fill,
+                                  adjacency);
     ++g_launches;
     k_csr_sort<<<g, 256, 0, st>>>(ws.miss, n, offsets, adjacency);
 }

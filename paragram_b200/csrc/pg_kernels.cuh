@@ -38,6 +38,10 @@ struct CellLaunch
     float *radius_out; // per original id: certified radius of the final cell, or nullptr
     int *work_out;     // per original id: nodes, leaves, candidates, peak queue; or nullptr
     float *geometry_out; // per original id: centroid x, y, z and volume of the cell; or nullptr
+    int vertex_cap;            // vertex export: slots per cell
+    float *vertices_out;       // per original id x vertex_cap: vertex relative to the point, error bound
+    int *vertex_planes_out;    // per original id x vertex_cap x 3: planes of the vertex (ids / -1 - box code)
+    int *vertex_count_out;     // per original id: number of vertices
     int use_hint;      // the workspace holds a search radius per sorted slot
     int fp32_only;     // side tests in FP32 only (no escalation; not exact)
 };

@@ -40,7 +40,7 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
          num_chunks: int = 0, stats: bool = False, profile: bool = False, blocks_per_sm: int = 0,
          diagnostics: bool = False, model: Optional[torch.Tensor] = None,
          radius_hint: Optional[torch.Tensor] = None, features: bool = False, fp32_only: bool = False,
-         geometry: bool = False):
+         geometry: bool = False, vertices: int = 0):
     n = int(points.shape[0])
     _check(points.device.type == "cuda", "points must be on CUDA device")
     _check(points.dtype == torch.float32, "points must be of type float")
@@ -90,6 +90,16 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
     if geometry:
         geom = torch.zeros(max(n, 1), 4, dtype=torch.float32, device=dev)
         opts.geometry_out = geom.data_ptr()
+    vtx = vpl = vcnt = None
+    if vertices:
+        _check(int(vertices) > 0, "vertices must be a positive capacity per cell")
+        cap = int(vertices)
+        vtx = torch.full((max(n, 1), cap, 4), float("nan"), dtype=torch.float32, device=dev)
+        vpl = torch.zeros(max(n, 1), cap, 3, dtype=torch.int32, device=dev)
+        vcnt = torch.zeros(max(n, 1), dtype=torch.int32, device=dev)
+        opts.vertex_cap = cap
+        opts.vertices_out, opts.vertex_planes_out, opts.vertex_count_out = (vtx.data_ptr(), vpl.data_ptr(),
+                                                                            vcnt.data_ptr())
     with torch.cuda.device(dev):
         nbytes = ctypes.c_size_t(0)
         rc = _LIB.pg_workspace_size(n, ctypes.byref(nbytes))
@@ -121,6 +131,9 @@ def _run(points: torch.Tensor, weights: Optional[torch.Tensor], knn: int, debug:
         _last_diag.update(features=feats[:n], order=order[:n])
     if geometry:
         _last_diag.update(centroids=geom[:n, :3], volumes=geom[:n, 3])
+    if vertices:
+        _last_diag.update(vertices=vtx[:n, :, :3], vertex_bound=vtx[:n, :, 3], vertex_planes=vpl[:n],
+                          vertex_count=vcnt[:n])
     return adjacency, offsets, status
 
 
@@ -150,7 +163,8 @@ def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = Non
                      initial_guesses: Optional[torch.Tensor] = None,
                      initial_guesses_offsets: Optional[torch.Tensor] = None, diagnostics: bool = False,
                      model: Optional[torch.Tensor] = None, radius_hint: Optional[torch.Tensor] = None,
-                     features: bool = False, fp32_only: bool = False, geometry: bool = False):
+                     features: bool = False, fp32_only: bool = False, geometry: bool = False,
+                     vertices: int = 0):
     """Build and return ``((adjacency, offsets, status), counters)``; counters as in ``STAT_NAMES``.
 
     With ``diagnostics=True`` the counters also hold ``radius`` (float32 [N], the certified radius
@@ -162,13 +176,18 @@ def build_with_stats(points: torch.Tensor, weights: Optional[torch.Tensor] = Non
     side test by its FP32 value (no FP64 / exact escalation; the result may differ from the exact
     diagram on near-degenerate input). With ``geometry=True`` the counters also hold ``centroids``
     (float32 [N, 3]) and ``volumes`` (float32 [N]) of the cells (empty cell: volume 0, NaN centroid).
+    With ``vertices=C`` (a capacity per cell) the counters also hold ``vertices`` (float32 [N, C, 3],
+    each cell's vertices relative to its point), ``vertex_bound`` (float32 [N, C]: a rigorous bound
+    on each vertex's distance from the exact vertex), ``vertex_planes`` (int32 [N, C, 3]: the planes
+    meeting there, as neighbour point indices or -1 - code for a box face, code = 2 * axis + 1 on
+    the high side) and ``vertex_count`` (int32 [N]); unused slots hold NaN / 0.
     """
     if weights is not None and weights.dim() == 1:
         weights = weights[:, None]
     res = _run(points, weights, knn, False, initial_guesses, initial_guesses_offsets, leaf_size,
                num_chunks=num_chunks, stats=True, profile=profile, blocks_per_sm=blocks_per_sm,
                diagnostics=diagnostics, model=model, radius_hint=radius_hint, features=features,
-               fp32_only=fp32_only, geometry=geometry)
+               fp32_only=fp32_only, geometry=geometry, vertices=vertices)
     out = dict(_last_stats)
     out.update(_last_diag)
     return res, out

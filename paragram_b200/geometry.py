@@ -36,4 +36,29 @@ def cell_geometry(points: torch.Tensor, weights: Optional[torch.Tensor] = None, 
     return Diagram(adjacency=adjacency, offsets=offsets, status=status), out["centroids"], out["volumes"]
 
 
-__all__ = ["cell_geometry"]
+def cell_vertices(points: torch.Tensor, weights: Optional[torch.Tensor] = None, *, capacity: int = 64,
+                  knn: int = 8, leaf_size: int = -1) -> Tuple[Diagram, dict]:
+    """Build the diagram and return ``(diagram, vertices)`` with every cell's vertices.
+
+    ``vertices`` holds ``count`` (int32 [N]: vertices of each cell, 0 for an empty cell),
+    ``positions`` (float32 [N, capacity, 3], absolute), ``relative`` (float32 [N, capacity, 3],
+    relative to the cell's point: the precision the builder works in), ``bound`` (float32
+    [N, capacity]: a rigorous bound on each vertex's distance from the exact vertex) and ``planes``
+    (int32 [N, capacity, 3]: the three planes meeting at the vertex, as neighbour point indices, or
+    -1 - code for a face of the bounding box, code = 2 * axis + 1 on the high side). A cell with
+    more than ``capacity`` vertices keeps its first ``capacity``; unused slots hold NaN / 0.
+    """
+    points = _validate_points(points)
+    if weights is not None:
+        weights = _validate_weights(weights, points.shape[0], points.device)
+    from .cuda import build_with_stats
+
+    (adjacency, offsets, status), out = build_with_stats(points, weights, knn=knn, leaf_size=leaf_size,
+                                                         vertices=capacity)
+    rel = out["vertices"]
+    verts = dict(count=out["vertex_count"], relative=rel, positions=rel + points[:, None, :],
+                 bound=out["vertex_bound"], planes=out["vertex_planes"])
+    return Diagram(adjacency=adjacency, offsets=offsets, status=status), verts
+
+
+__all__ = ["cell_geometry", "cell_vertices"]

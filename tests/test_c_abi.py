@@ -82,3 +82,40 @@ def test_mlp_entry_points_without_gpu(lib):
     assert lib.pg_mlp_adam(None, None, None, None, 1, 1e-3, 0.9, 0.999, 1e-8, None, None) == -1
     assert lib.pg_mlp_adam(256, 256, 256, 256, 0, 1e-3, 0.9, 0.999, 1e-8, 256, None) == -1  # step must be >= 1
     assert lib.pg_mlp_pack(None, None, None) == -1
+
+
+def test_vertex_export_arguments(lib):
+    from paragram_b200 import _lib
+
+    opt = _lib.PgOptions(8, -1, 0, 0)
+    opt.vertices_out = 256  # vertex_cap 0 with an output
+    assert _build(lib, 10, options=opt) == -1
+    assert "vertex_cap" in _lib.last_error(lib)
+    opt.vertex_cap = 8
+    opt.vertices_out = 264  # float4 rows need 16-byte alignment
+    assert _build(lib, 10, options=opt) == -1
+    assert "vertices_out" in _lib.last_error(lib)
+    opt.vertex_cap = -1
+    opt.vertices_out = None
+    assert _build(lib, 10, options=opt) == -1
+
+
+def test_options_layout_matches_header(tmp_path):
+    """The ctypes mirror of pg_options has the header's size and field offsets."""
+    import shutil
+    import subprocess
+
+    from paragram_b200 import _lib
+
+    if shutil.which("gcc") is None:
+        pytest.skip("needs gcc")
+    fields = [f for f, _ in _lib.PgOptions._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "paragram_b200.h"\nint main(void){\n'
+                   '  printf("%zu\\n", sizeof(pg_options));\n' +
+                   "".join(f'  printf("%zu\\n", offsetof(pg_options, {f}));\n' for f in fields) + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", f"-I{os.path.join(ROOT, 'include')}", str(src), "-o", str(exe)], check=True)
+    vals = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert vals[0] == ctypes.sizeof(_lib.PgOptions)
+    assert vals[1:] == [getattr(_lib.PgOptions, f).offset for f in fields]

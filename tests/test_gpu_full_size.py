@@ -16,6 +16,7 @@ import time
 import numpy as np
 import pytest
 import torch
+from _helpers import diff_cells as _diff_cells
 
 pytestmark = pytest.mark.gpu
 
@@ -29,25 +30,6 @@ def dev():
 
 def _np(d):
     return d.adjacency.cpu().numpy(), d.offsets.cpu().numpy(), d.status.cpu().numpy()
-
-
-def _diff_cells(got, exp):
-    """Indices of the cells whose sorted row or status differ."""
-    adj, off, st = got
-    eadj, eoff, est = exp
-    deg, edeg = np.diff(off.astype(np.int64)), np.diff(eoff.astype(np.int64))
-    bad = (st != est) | (deg != edeg)
-    same = ~bad
-    # rows of cells with equal degree: compare entry by entry
-    rows = np.repeat(np.arange(len(st)), deg)
-    erows = np.repeat(np.arange(len(st)), edeg)
-    keep = same[rows]
-    keep_e = same[erows]
-    a, b = adj[keep], eadj[keep_e]
-    r = rows[keep]
-    if a.size:
-        bad[np.unique(r[a != b])] = True
-    return np.flatnonzero(bad)
 
 
 def _oracle(oracle, pts, w=None):

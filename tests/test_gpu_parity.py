@@ -289,3 +289,23 @@ def test_fp32_only_predicates(dev, oracle):
         (a, o, s), st = pc.build_with_stats(t, tw, fp32_only=True)
         assert st["fp64_escalations"] == 0 and st["exact_escalations"] == 0
         _assert_same((a.cpu().numpy(), o.cpu().numpy(), s.cpu().numpy()), oracle.diagram(pts, w), "fp32 only")
+
+
+@pytest.mark.parametrize("env", [{"PARAGRAM_NUM_CHUNKS": "4"}, {"PARAGRAM_MEM_FRAC": "0.06"},
+                                 {"PARAGRAM_NUM_CHUNKS": "0", "PARAGRAM_MEM_FRAC": "2.0"}])
+def test_chunk_environment(dev, monkeypatch, env):
+    """The reference's chunk-plan environment (chunking.h:16-37) splits the cell pass into launches;
+    the diagram is identical. PARAGRAM_MEM_FRAC outside (0.05, 0.95) is ignored, as in the reference."""
+    import paragram_b200.cuda as pc
+    from paragram_b200 import workloads as W
+
+    pts = W.clustered(40_000, seed=17)
+    t = torch.from_numpy(pts).to(dev)
+    base = [x.cpu() for x in pc.build_with_stats(t)[0]]
+    for k, v in env.items():
+        monkeypatch.setenv(k, v)
+    got = [x.cpu() for x in pc.build_with_stats(t, profile=True)[0]]
+    assert all(torch.equal(a, b) for a, b in zip(base, got))
+    chunks = pc.last_profile()["chunks"]
+    if env.get("PARAGRAM_NUM_CHUNKS") == "4":
+        assert chunks == 4
