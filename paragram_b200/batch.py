@@ -63,8 +63,15 @@ class _Static:
 
 
 def build_batch(points: Sequence[torch.Tensor], weights: Optional[Sequence[torch.Tensor]] = None, *,
-                leaf_size: int = -1, graph: bool = False, blocks_per_sm: int = 0) -> list[Diagram]:
-    """Diagrams of independent clouds (Voronoi, or power when ``weights`` is given) in one build."""
+                leaf_size: int = -1, graph: bool = False, blocks_per_sm: int = 0, model=None,
+                geometry_out: Optional[torch.Tensor] = None) -> list[Diagram]:
+    """Diagrams of independent clouds (Voronoi, or power when ``weights`` is given) in one build.
+
+    ``model``: a trained ``paragram_b200.learned.Model`` (its search radius per point, predicted for
+    every cloud in the same launch); the diagrams do not depend on it. ``geometry_out``: a float32
+    [total points, 4] CUDA tensor (clouds concatenated in order) that receives each cell's
+    centroid (x, y, z) and volume, as ``paragram_b200.cell_geometry`` does for one cloud.
+    """
     if len(points) == 0:
         return []
     lib = _lib.load()
@@ -80,8 +87,26 @@ def build_batch(points: Sequence[torch.Tensor], weights: Optional[Sequence[torch
             if w.device != dev or w.dtype != torch.float32 or w.numel() != p.shape[0]:
                 raise ValueError("weights must be float32 with one entry per point, on the points' device")
     sizes = tuple(int(p.shape[0]) for p in points)
-    key = (dev.index, sizes, weights is not None, int(leaf_size), int(blocks_per_sm))
+    blob = None
+    if model is not None:
+        blob = model.blob
+        if blob.device != dev:
+            raise ValueError("the model must live on the clouds' device")
+    total_points = int(sum(int(p.shape[0]) for p in points))
+    if geometry_out is not None:
+        if not (isinstance(geometry_out, torch.Tensor) and geometry_out.device == dev and
+                geometry_out.dtype == torch.float32 and geometry_out.is_contiguous() and
+                tuple(geometry_out.shape) == (total_points, 4)):
+            raise ValueError("geometry_out must be a contiguous float32 (total points, 4) tensor on the clouds' device")
+    # a captured graph holds the model's and geometry's device addresses: they are part of the key
+    key = (dev.index, tuple(int(p.shape[0]) for p in points), weights is not None, int(leaf_size),
+           int(blocks_per_sm), None if blob is None else blob.data_ptr(),
+           None if geometry_out is None else geometry_out.data_ptr())
     opts = _lib.PgOptions(8, int(leaf_size), 0, 0, int(blocks_per_sm))
+    if blob is not None:
+        opts.model = blob.data_ptr()
+    if geometry_out is not None and total_points > 0:
+        opts.geometry_out = geometry_out.data_ptr()
     with torch.cuda.device(dev):
         st = _graphs.get(key) if graph else None
         if st is None:

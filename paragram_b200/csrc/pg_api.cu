@@ -73,7 +73,6 @@ size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
     w.flags = (int *)take(4 * N);
     w.nbox = (float4 *)take(32 * N);
     w.records = (float4 *)take(64 * N);
-    w.region = (float4 *)take(32 * N);
     w.rparent = (int *)take(4 * N);
     w.pleaf = (int *)take(4 * N);
     w.hint = (float *)take(4 * N);

@@ -82,38 +82,20 @@ template <int CAP, int STACK> struct CellMem
     float vr[CAP];    // (|X| + psi)^2, upper bound on |X_exact|^2
     int pid[CAP];     // >= 0: sorted point index; < 0: -1 - box code
     unsigned vt[CAP]; // plane slots of the vertex, tri_pack(p0, p1, p2) (oriented)
-    unsigned eb[CAP]; // boundary edges x | y << 10 | w << 20 of the clip in progress, by rank
-    // lk[e][v]: the vertex across the dual edge e of vertex v (e = 0: p0 -> p1, 1: p1 -> p2,
-    // 2: p2 -> p0), i.e. the vertex holding the reverse plane pair: the polytope's edges
-    using Slot = typename std::conditional<(CAP <= 256), unsigned char, unsigned short>::type;
-    Slot lk[3][CAP];
-    Slot bst[CAP], ben[CAP]; // new vertex whose boundary edge starts / ends at a plane
+    unsigned eb[CAP]; // boundary edges x | y << 16 of the clip in progress, by rank
     int stk[STACK];   // pending BVH references (unordered)
     float skey[STACK]; // lower bound of the bisector distance of any point of the pending node
     unsigned long long cnt[kNumStats]; // per-warp statistics (written by lane 0)
     unsigned long long cnt0[3];        // nodes, leaves, candidates at the start of the current cell
+    unsigned et[CAP * CAP / 32];       // edge table of the clip in progress (all zero between clips)
 };
 
-// Give a warp's boundary tables in-range contents (once, before its first clip).
+// Clear a warp's edge table (once, before its first clip).
 template <int CAP, int STACK> __device__ __forceinline__ void clear_edges(CellMem<CAP, STACK> &m, int lane)
 {
-    for (int k = lane; k < CAP; k += 32)
-    {
-        m.bst[k] = 0;
-        m.ben[k] = 0;
-    }
+    for (int k = lane; k < CAP * CAP / 32; k += 32)
+        m.et[k] = 0u;
     __syncwarp();
-}
-
-// Bit s of a per-word slot mask.
-template <int W> __device__ __forceinline__ unsigned mask_bit(const unsigned (&mk)[W], unsigned s)
-{
-    unsigned word = 0;
-#pragma unroll(W > 8 ? 1 : W)
-    for (int kk = 0; kk < W; ++kk)
-        if ((int)(s >> 5) == kk)
-            word = mk[kk];
-    return (word >> (s & 31u)) & 1u;
 }
 
 struct CellArgs
@@ -152,7 +134,6 @@ struct CellArgs
     const float *hint; // search radius per sorted slot (learned or given), or nullptr
     const int *rparent; // record node -> entry in its parent's record
     const int *pleaf;   // sorted point -> entry of its leaf
-    const float4 *region; // key-prefix region of each record node (lo, hi)
     int fp32_only;      // undecided FP32 side tests take the FP32 sign (no exact cascade)
 };
 
@@ -430,11 +411,6 @@ __device__ __forceinline__ void cell_init(CellMem<CAP, STACK> &m, WarpState<CAP>
         m.vx[lane] = make_float4(X, Y, Z, psi);
         m.vr[lane] = rr * rr * (1.0f + 1e-6f);
         m.vt[lane] = tri_pack((unsigned)p0, (unsigned)p1, (unsigned)p2);
-        // the corner across dual edge e shares its two planes and differs along the third's axis
-        const int tp[3] = {p0, p1, p2};
-#pragma unroll
-        for (int e = 0; e < 3; ++e)
-            m.lk[e][lane] = (typename CellMem<CAP, STACK>::Slot)(lane ^ (1 << (tp[(e + 2) % 3] >> 1)));
     }
     __syncwarp();
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
@@ -626,27 +602,48 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         m.pe[P] = q.eh;
         m.pid[P] = q.id;
     }
-    // boundary edges of the removed region: the dual edge x->y of a removed vertex
-    // is a boundary edge iff the vertex across it (holding y->x) is kept; the new
-    // face gets one vertex (P, x, y) per boundary edge, on the polytope edge from
-    // the removed vertex to that kept one. The reference walks the same boundary
-    // sequentially (CCComputeBoundary, faster_convex_cell.cuh:322-388).
+    // boundary edges of the removed region: the directed edge x->y of a removed
+    // triangle is a boundary edge iff y->x is not an edge of another removed
+    // triangle. The removed triangles mark their edges in the warp's edge table
+    // (bit x * CAP + y), each lane tests the reverses of its own edges, then the
+    // marks are cleared (the table is all zero between clips).
     using Bits = typename std::conditional<(3 * W > 32), unsigned long long, unsigned>::type;
     Bits bf = 0; // bit k*3+e: edge e of my removed vertex in word k is a boundary edge
-    unsigned kept[W][3]; // the kept vertex across that edge
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
-#pragma unroll
-        for (int e = 0; e < 3; ++e)
+        if ((rem[k] >> lane) & 1u)
         {
-            kept[k][e] = 0;
-            if ((rem[k] >> lane) & 1u)
+            unsigned t = tri[k];
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
             {
-                unsigned nbv = m.lk[e][k * 32 + lane];
-                kept[k][e] = nbv;
-                if (!mask_bit(rem, nbv))
+                unsigned bit = tri_get(t, e) * CAP + tri_get(t, (e + 1) % 3);
+                atomicOr(&m.et[bit >> 5], 1u << (bit & 31u));
+            }
+        }
+    __syncwarp();
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+        if ((rem[k] >> lane) & 1u)
+        {
+            unsigned t = tri[k];
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+            {
+                unsigned rbit = tri_get(t, (e + 1) % 3) * CAP + tri_get(t, e);
+                if (!((m.et[rbit >> 5] >> (rbit & 31u)) & 1u))
                     bf |= (Bits)1u << (3 * k + e);
             }
+        }
+    __syncwarp();
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+        if ((rem[k] >> lane) & 1u)
+        {
+            unsigned t = tri[k];
+#pragma unroll
+            for (int e = 0; e < 3; ++e)
+                m.et[(tri_get(t, e) * CAP + tri_get(t, (e + 1) % 3)) >> 5] = 0u;
         }
     // list the boundary edges in the warp's edge buffer, lane by lane (exclusive scan of the counts)
     int mine = 0;
@@ -670,7 +667,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
             if ((bf >> f) & 1u)
             {
                 unsigned my = tri[f / 3];
-                m.eb[at++] = tri_get(my, f % 3) | (tri_get(my, (f % 3 + 1) % 3) << 10) | (kept[f / 3][f % 3] << 20);
+                m.eb[at++] = tri_get(my, f % 3) | (tri_get(my, (f % 3 + 1) % 3) << 16);
             }
     }
     int nv_new = count_bits(ws.valid) - count_bits(rem) + nb;
@@ -695,7 +692,7 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
         if (r < nb)
         {
             unsigned xy = m.eb[r];
-            unsigned x = xy & 1023u, y = (xy >> 10) & 1023u;
+            unsigned x = xy & 0xFFFFu, y = xy >> 16;
             int rr = r, slot = -1;
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
             for (int k = 0; k < W; ++k)
@@ -714,8 +711,6 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
                 m.vx[slot] = X;
                 m.vr[slot] = vr;
                 m.vt[slot] = tri_pack((unsigned)P, x, y);
-                m.bst[x] = (typename CellMem<CAP, STACK>::Slot)slot;
-                m.ben[y] = (typename CellMem<CAP, STACK>::Slot)slot;
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
                 for (int k = 0; k < W; ++k)
                     if ((slot >> 5) == k)
@@ -723,30 +718,6 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
             }
             else
                 ws.flags |= kFlagError; // unreachable: capacity was checked above
-        }
-    }
-    __syncwarp();
-    // links of the new vertices: (P, x, y) borders the new vertex whose boundary edge
-    // ends at x (across P->x), the kept vertex w (across x->y) and the new vertex whose
-    // boundary edge starts at y (across y->P); w's link across y->x now ends at it
-    for (int r0 = 0; r0 < nb; r0 += 32)
-    {
-        int r = r0 + lane;
-        if (r < nb)
-        {
-            unsigned xyw = m.eb[r];
-            unsigned x = xyw & 1023u, y = (xyw >> 10) & 1023u, w = xyw >> 20;
-            unsigned slot = m.bst[x], nxt = m.bst[y];
-            m.lk[0][slot] = m.ben[x];
-            m.lk[1][slot] = (typename CellMem<CAP, STACK>::Slot)w;
-            m.lk[2][slot] = (typename CellMem<CAP, STACK>::Slot)nxt;
-            unsigned tw = m.vt[w];
-            int ew = (tri_get(tw, 0) == y && tri_get(tw, 1) == x) ? 0 : ((tri_get(tw, 1) == y && tri_get(tw, 2) == x) ? 1 : 2);
-            if (ew == 2 && !(tri_get(tw, 2) == y && tri_get(tw, 0) == x))
-                ws.flags |= kFlagError; // unreachable: the boundary of a convex cut is one cycle
-            m.lk[ew][w] = (typename CellMem<CAP, STACK>::Slot)slot;
-            if (tri_get(m.vt[nxt], 1) != y)
-                ws.flags |= kFlagError; // unreachable, as above
         }
     }
     // ill-conditioned in FP32: rebuild in FP64 so that the empty sphere stays tight
@@ -873,27 +844,6 @@ __device__ __forceinline__ bool box_key(const WarpState<CAP> &ws, float lx, floa
     }
     key = t * (1.0f - 1e-5f);
     return !(key > ws.rsafe);
-}
-
-// Lower bound of the bisector distance of any point of a cloud whose points weigh at
-// most mw and lie at least D (itself a lower bound) from the seed; +inf for D = +inf.
-template <int CAP> __device__ __forceinline__ float dist_key(const WarpState<CAP> &ws, float D, float mw)
-{
-    if (!(D > 0.0f))
-        return 0.0f;
-    if (D == INFINITY)
-        return INFINITY;
-    float d = D * (1.0f - 4e-6f);
-    float dm = mw - ws.s.w;
-    float t;
-    if (dm <= 0.0f)
-        t = 0.5f * d;
-    else
-    {
-        float num = d * d * (1.0f - 1e-6f) - dm * (1.0f + 1e-6f);
-        t = num > 0.0f ? __fdividef(num, 2.0f * d) * (1.0f - 4e-6f) : 0.0f;
-    }
-    return t * (1.0f - 1e-5f);
 }
 
 // Vertices whose empty sphere reaches the box: q in the box can remove v only
@@ -1063,77 +1013,6 @@ __device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP
     return run_batch(m, ws, have, q, qkey, A, lane, vm, true);
 }
 
-// One step up the seed's path to its cloud's root. Entry e = (parent << 1 | side)
-// is a node whose points are queued or done: queue its sibling (with its box
-// bound) and, unless parent is the cloud's root, a continuation entry -3 -
-// parent whose bound covers every point outside parent's subtree (those lie
-// outside parent's key-prefix region, whose distance from the seed bounds
-// them). The path is climbed only as far as those bounds stay within the cell's
-// radius. Returns the new queue length.
-template <int CAP, int STACK, bool HINT>
-__device__ __forceinline__ int climb(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, const CellArgs &A, int lane, int e,
-                                    int sp, float cap, bool &capped)
-{
-    int parent = e >> 1, side = e & 1;
-    if (e < 0 || parent >= A.n - 1)
-    {
-        ws.flags |= kFlagError; // unreachable: the path always meets the cloud's root
-        return sp;
-    }
-    if (sp + 2 > STACK)
-    {
-        ws.flags |= kFlagDefer;
-        PG_COUNT(m, lane, kStatDeferStack, 1);
-        return sp;
-    }
-    const float4 *r = A.rec + 4 * (size_t)parent;
-    float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
-    float k;
-    bool p = side == 1 ? box_key(ws, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r3.z, k)
-                       : box_key(ws, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.w, k);
-    if (HINT)
-    {
-        capped = capped || (p && k > cap);
-        p = p && !(k > cap);
-    }
-    if (p)
-    {
-        if (lane == 0)
-        {
-            m.stk[sp] = (parent << 1) | (side ^ 1);
-            m.skey[sp] = k;
-        }
-        ++sp;
-    }
-    if (parent != ws.root)
-    {
-        float4 rl = A.region[2 * (size_t)parent], rh = A.region[2 * (size_t)parent + 1];
-        float D = 0.0f;
-        if (rl.w == 0.0f)
-            D = fmaxf(fminf(fminf(fminf(ws.s.x - rl.x, rh.x - ws.s.x), fminf(ws.s.y - rl.y, rh.y - ws.s.y)),
-                            fminf(ws.s.z - rl.z, rh.z - ws.s.z)),
-                      0.0f);
-        float kc = dist_key(ws, D, ws.box[6]);
-        bool pc = true;
-        if (HINT)
-        {
-            capped = capped || kc > cap;
-            pc = !(kc > cap);
-        }
-        if (pc)
-        {
-            if (lane == 0)
-            {
-                m.stk[sp] = -3 - parent;
-                m.skey[sp] = kc;
-            }
-            ++sp;
-        }
-    }
-    ws.peak = max(ws.peak, sp);
-    return sp;
-}
-
 // Best-first BVH traversal of one cell. A pending entry is (parent << 1 | side)
 // with a lower bound of the bisector distance of the child's points; the
 // entry with the smallest bound is popped, dropped if the bound exceeds the
@@ -1147,10 +1026,10 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
                                          float cap, float done_cap, bool &capped)
 {
     const float4 *rec = A.rec;
-    // Start at the seed's own leaf (bound 0), its sibling and a continuation up
-    // the path to the cloud's root (climb), instead of descending from the
-    // root. A cloud whose root is a leaf starts with entry -2 (that leaf,
-    // unbounded box).
+    // Start at the seed's own leaf (bound 0) and queue the sibling of every node
+    // on its path up to the cloud's root with its bound, instead of descending
+    // from the root. A cloud whose root is a leaf starts with entry -2 (that
+    // leaf, unbounded box).
     int sp = 1;
     if (ref_is_leaf(ws.root))
     {
@@ -1168,9 +1047,37 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
             m.stk[0] = e;
             m.skey[0] = 0.0f;
         }
-        sp = climb<CAP, STACK, HINT>(m, ws, A, lane, e, sp, cap, capped);
-        if (ws.flags & kFlagDefer)
-            return false;
+        for (int lvl = 0; lvl < STACK - 1; ++lvl)
+        {
+            int parent = e >> 1, side = e & 1;
+            if (e < 0 || parent >= A.n - 1)
+            {
+                ws.flags |= kFlagError; // unreachable: the path always meets the cloud's root
+                break;
+            }
+            const float4 *r = rec + 4 * (size_t)parent;
+            float4 r0 = r[0], r1 = r[1], r2 = r[2], r3 = r[3];
+            float k;
+            bool p = side == 1 ? box_key(ws, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r3.z, k)
+                               : box_key(ws, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.w, k);
+            if (HINT)
+            {
+                capped = capped || (p && k > cap);
+                p = p && !(k > cap);
+            }
+            if (p)
+            {
+                if (lane == 0)
+                {
+                    m.stk[sp] = (parent << 1) | (side ^ 1);
+                    m.skey[sp] = k;
+                }
+                ++sp;
+            }
+            if (parent == ws.root)
+                break;
+            e = A.rparent[parent];
+        }
     }
     ws.peak = max(ws.peak, sp);
     __syncwarp();
@@ -1212,16 +1119,6 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
             capped = true;
             if (floor_key > cap)
                 break;
-            continue;
-        }
-        if (ent <= -3)
-        {
-            // continuation: one more step up the seed's path
-            sp = climb<CAP, STACK, HINT>(m, ws, A, lane, A.rparent[-3 - ent], sp, cap, capped);
-            __syncwarp();
-            PG_T1(m, lane, kStatCycNodes, tn);
-            if (ws.flags & kFlagDefer)
-                return false;
             continue;
         }
         PG_COUNT(m, lane, kStatNodes, 1);
@@ -1432,10 +1329,9 @@ __device__ __noinline__ float4 vertex64_plain(int pid0, int pid1, int pid2, cons
 // triangle holds the directed pair a -> c, and all terms share one sign.
 // Writes (centroid x, y, z, volume); a deferred cell writes NaN (the larger
 // pass overwrites it), an empty cell volume 0 and a NaN centroid.
-// (not inlined: the cell kernels keep their register allocation when no geometry is asked for;
-// the valid-slot masks arrive in m.eb, free once the cell is final)
+// (the valid-slot masks arrive in m.eb, free once the cell is final)
 template <int CAP, int STACK>
-__device__ __noinline__ void integrate_cell(CellMem<CAP, STACK> &m, const CellArgs &A, int lane, int soid, float4 s,
+__device__ __forceinline__ void integrate_cell(CellMem<CAP, STACK> &m, const CellArgs &A, int lane, int soid, float4 s,
                                             const float *box)
 {
     constexpr int W = WarpState<CAP>::W;
@@ -1443,6 +1339,39 @@ __device__ __noinline__ void integrate_cell(CellMem<CAP, STACK> &m, const CellAr
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < W; ++k)
         valid[k] = m.eb[k];
+    // the directed plane pair (a -> c) that each of this lane's vertices needs, per rotation
+    unsigned want[W][3];
+    int succ[W][3];
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int k = 0; k < W; ++k)
+    {
+        unsigned t = m.vt[k * 32 + lane];
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+        {
+            want[k][r] = ((valid[k] >> lane) & 1u) ? (tri_get(t, r) << 10 | tri_get(t, (r + 2) % 3)) : ~0u;
+            succ[k][r] = -1;
+        }
+    }
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+    for (int kj = 0; kj < W; ++kj)
+    {
+        unsigned vm = valid[kj];
+        while (vm)
+        {
+            int j = kj * 32 + __ffs(vm) - 1;
+            vm &= vm - 1;
+            unsigned tj = m.vt[j];
+            unsigned x0 = tri_get(tj, 0), x1 = tri_get(tj, 1), x2 = tri_get(tj, 2);
+            unsigned e0 = x0 << 10 | x1, e1 = x1 << 10 | x2, e2 = x2 << 10 | x0;
+#pragma unroll(CAP > 256 ? 1 : CAP / 32)
+            for (int k = 0; k < W; ++k)
+#pragma unroll
+                for (int r = 0; r < 3; ++r)
+                    if (want[k][r] == e0 || want[k][r] == e1 || want[k][r] == e2)
+                        succ[k][r] = j;
+        }
+    }
     // The FP32 vertices are only as accurate as the side tests need (psi); rebuild in FP64 the
     // ones whose bound exceeds 32 ulps of their size, so that each vertex is within about
     // 2^-19 |v| of the exact one (a power cell far from its seed amplifies that by |v| / size).
@@ -1499,9 +1428,10 @@ __device__ __noinline__ void integrate_cell(CellMem<CAP, STACK> &m, const CellAr
 #pragma unroll
         for (int r = 0; r < 3; ++r)
         {
-            // the edge of face a = p_r leaving this vertex ends at the vertex across p_{r+2} -> p_r
+            if (succ[k][r] < 0)
+                continue;
             float4 p = m.pl[tri_get(t, r)];
-            float4 u = m.vx[m.lk[(r + 2) % 3][slot]];
+            float4 u = m.vx[succ[k][r]];
             u.x -= ox;
             u.y -= oy;
             u.z -= oz;
@@ -1533,45 +1463,19 @@ __device__ __noinline__ void integrate_cell(CellMem<CAP, STACK> &m, const CellAr
     }
 }
 
+// Vertex export of a final cell: its valid vertices (masks in m.eb) in slot
+// order, relative to the seed with their error radius psi, which bounds the
+// distance to the exact vertex, and their planes as original point ids (box
+// planes -1 - code).
 template <int CAP, int STACK>
-__device__ __forceinline__ void write_geometry(CellMem<CAP, STACK> &m, const WarpState<CAP> &ws,
-                                               const CellArgs &A, int lane)
-{
-    constexpr int W = WarpState<CAP>::W;
-    if (ws.flags & (kFlagDefer | kFlagEmpty))
-    {
-        if (lane == 0)
-        {
-            float nan = __int_as_float(0x7fc00000);
-            A.geometry_out[ws.soid] = make_float4(nan, nan, nan, (ws.flags & kFlagDefer) ? nan : 0.0f);
-        }
-        return;
-    }
-    if (lane == 0)
-    {
-#pragma unroll(CAP > 256 ? 1 : CAP / 32)
-        for (int k = 0; k < W; ++k)
-            m.eb[k] = ws.valid[k];
-    }
-    __syncwarp();
-    integrate_cell(m, A, lane, ws.soid, ws.s, ws.box);
-}
-
-// Vertex export of a final cell: its valid vertices in slot order (relative to
-// the seed, with their error radius psi, which bounds the distance to the exact
-// vertex) and their planes as original point ids (box planes -1 - code).
-// A cell deferred to the larger pass writes nothing here (that pass does).
-// (not inlined: the cell kernels keep their register allocation)
-template <int CAP, int STACK>
-__device__ __noinline__ void write_vertices(CellMem<CAP, STACK> &m, const unsigned *valid, const CellArgs &A,
-                                            int lane, int soid)
+__device__ __forceinline__ void write_vertices(CellMem<CAP, STACK> &m, const CellArgs &A, int lane, int soid)
 {
     constexpr int W = WarpState<CAP>::W;
     const int cap = A.vertex_cap;
     int base = 0;
     for (int k = 0; k < W; ++k)
     {
-        unsigned v = valid[k];
+        unsigned v = m.eb[k];
         if ((v >> lane) & 1u)
         {
             int rank = base + __popc(v & ((1u << lane) - 1u));
@@ -1598,21 +1502,49 @@ __device__ __noinline__ void write_vertices(CellMem<CAP, STACK> &m, const unsign
         A.vertex_count_out[soid] = base;
 }
 
+// Geometry and vertex export of a final cell (valid-slot masks in m.eb). A cell
+// deferred to the larger pass writes NaN geometry and no vertices (that pass
+// writes them); an empty cell volume 0, a NaN centroid and no vertices.
+// (one non-inlined call site: the cell kernels keep their register allocation
+// and code size when no export is asked for)
+template <int CAP, int STACK>
+__device__ __noinline__ void export_cell(CellMem<CAP, STACK> &m, const CellArgs &A, int lane, int soid, float4 s,
+                                         const float *box, int flags)
+{
+    if (A.geometry_out != nullptr)
+    {
+        if (flags & (kFlagDefer | kFlagEmpty))
+        {
+            if (lane == 0)
+            {
+                float nan = __int_as_float(0x7fc00000);
+                A.geometry_out[soid] = make_float4(nan, nan, nan, (flags & kFlagDefer) ? nan : 0.0f);
+            }
+        }
+        else
+            integrate_cell(m, A, lane, soid, s, box);
+    }
+    if ((A.vertex_count_out != nullptr || A.vertices_out != nullptr || A.vertex_planes_out != nullptr) &&
+        !(flags & kFlagDefer))
+        write_vertices(m, A, lane, soid); // after the integration, which may refine vertices in place
+}
+
 template <int CAP, int STACK>
 __device__ __forceinline__ void write_diagnostics(CellMem<CAP, STACK> &m, const WarpState<CAP> &ws,
                                                   const CellArgs &A, int lane)
 {
-    if (A.geometry_out != nullptr)
-        write_geometry(m, ws, A, lane);
-    if ((A.vertex_count_out != nullptr || A.vertices_out != nullptr || A.vertex_planes_out != nullptr) &&
-        !(ws.flags & kFlagDefer))
+    constexpr int W = WarpState<CAP>::W;
+    if (A.geometry_out != nullptr || A.vertex_count_out != nullptr || A.vertices_out != nullptr ||
+        A.vertex_planes_out != nullptr)
     {
-        // the geometry pass above may have refined the vertices in place: export what the cell holds
-        unsigned valid[WarpState<CAP>::W];
+        if (lane == 0)
+        {
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
-        for (int k = 0; k < WarpState<CAP>::W; ++k)
-            valid[k] = (ws.flags & kFlagEmpty) ? 0u : ws.valid[k];
-        write_vertices(m, valid, A, lane, ws.soid);
+            for (int k = 0; k < W; ++k)
+                m.eb[k] = ws.valid[k];
+        }
+        __syncwarp();
+        export_cell(m, A, lane, ws.soid, ws.s, ws.box, ws.flags);
     }
     if (lane != 0)
         return;
@@ -1773,7 +1705,6 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.rparent = ws.rparent;
     A.fp32_only = cl.fp32_only;
     A.pleaf = ws.pleaf;
-    A.region = ws.region;
     return A;
 }
 

@@ -131,7 +131,6 @@ struct Workspace
     int *flags;           // [N] refit arrival counters
     float4 *nbox;         // [2N] internal node box lo(xyz)+maxw, hi(xyz)+count
     float4 *records;      // [4N] traversal records of internal nodes
-    float4 *region;       // [2N] key-prefix region of each record node (lo, hi), see k_records
     int *rparent;         // [N] record node -> its entry in its parent's record (parent << 1 | side)
     int *pleaf;           // [N] sorted point -> the entry of the leaf holding it (parent << 1 | side)
     float *hint;          // [N] search radius per sorted slot (learned or given), <= 0: none

@@ -366,67 +366,14 @@ __global__ void k_refit(const float4 *__restrict__ pts, int64_t n, const int *__
     }
 }
 
-// Region of the curve (key prefix) that internal node i's points fill: every
-// point of the cloud outside i's subtree has another key prefix, so it lies
-// outside this box (Karras ranges are exactly the keys sharing the node's
-// prefix). reg[2i] = (lo x, y, z, 1 if no bound), reg[2i+1] = (hi x, y, z):
-// faces where the prefix reaches the cloud's Morton frame are open (+-inf),
-// and each closed face is moved inward by a margin that covers the rounding of
-// the key quantisation and of the distances measured to it. A node whose keys
-// are all equal (the index breaks the tie) gives no bound.
-__device__ __forceinline__ void node_region(const unsigned long long *__restrict__ keys, int lo_i, int hi_i, int bits,
-                                            const float *__restrict__ morton, float4 &rlo, float4 &rhi)
-{
-    unsigned long long ka = keys[lo_i], kb = keys[hi_i];
-    rlo = make_float4(-INFINITY, -INFINITY, -INFINITY, 1.0f);
-    rhi = make_float4(INFINITY, INFINITY, INFINITY, 0.0f);
-    if (ka == kb)
-        return;
-    const int mb = 3 * bits;                          // Morton bits below the cloud id
-    int fixed = __clzll(ka ^ kb) - (64 - mb);         // Morton bits shared by the node's keys
-    if (fixed < 0)
-        return;
-    int c = (int)(ka >> mb);
-    float o[3] = {morton[c * 4 + 0], morton[c * 4 + 1], morton[c * 4 + 2]};
-    float ext = morton[c * 4 + 3];
-    unsigned top = (1u << bits) - 1u;
-    float cell = ext > 0.0f ? ext / (float)top : 0.0f;
-    float lo[3], hi[3];
-    for (int a = 0; a < 3; ++a)
-    {
-        // bits of axis a sit at positions 3 b + (2 - a); count and read those within the prefix
-        int n = 0;
-        unsigned v = 0;
-        for (int b = bits - 1; b >= 0; --b)
-        {
-            int pos = 3 * b + (2 - a);
-            if (pos < mb - fixed)
-                break;
-            v = (v << 1) | (unsigned)((ka >> pos) & 1ull);
-            ++n;
-        }
-        unsigned qlo = n > 0 ? v << (bits - n) : 0u;
-        unsigned qhi = n > 0 ? ((v + 1u) << (bits - n)) - 1u : top;
-        // margin: the key quantisation's rounding (under one cell) plus the rounding of these face
-        // positions and of the traversal's distances to them (a few ulps of the frame's coordinates)
-        float mg = 2.0f * cell + 8e-7f * (fabsf(o[a]) + ext);
-        lo[a] = qlo == 0u ? -INFINITY : o[a] + (float)qlo * cell + mg;
-        hi[a] = qhi >= top ? INFINITY : o[a] + (float)(qhi + 1u) * cell - mg;
-    }
-    rlo = make_float4(lo[0], lo[1], lo[2], 0.0f);
-    rhi = make_float4(hi[0], hi[1], hi[2], 0.0f);
-}
-
 // Traversal record of internal node i (only nodes with > leaf points are read):
 //   r0 = (c0.lo.x, c0.lo.y, c0.lo.z, c0.hi.x)
 //   r1 = (c0.hi.y, c0.hi.z, c1.lo.x, c1.lo.y)
 //   r2 = (c1.lo.z, c1.hi.x, c1.hi.y, c1.hi.z)
 //   r3 = (ref0, ref1, maxw0, maxw1)
 __global__ void k_records(const float4 *__restrict__ pts, int64_t n, const int *__restrict__ left,
-                          const int *__restrict__ right, const int *__restrict__ first, const int *__restrict__ last,
-                          const float4 *__restrict__ nbox, const unsigned long long *__restrict__ keys, int bits,
-                          const float *__restrict__ morton, int leaf, float4 *__restrict__ rec,
-                          float4 *__restrict__ reg, int *__restrict__ rparent, int *__restrict__ pleaf)
+                          const int *__restrict__ right, const int *__restrict__ first, const float4 *__restrict__ nbox,
+                          int leaf, float4 *__restrict__ rec, int *__restrict__ rparent, int *__restrict__ pleaf)
 {
     int64_t ii = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (ii >= n - 1)
@@ -459,10 +406,6 @@ __global__ void k_records(const float4 *__restrict__ pts, int64_t n, const int *
     rec[4 * (size_t)i + 1] = make_float4(chi[0].y, chi[0].z, clo[1].x, clo[1].y);
     rec[4 * (size_t)i + 2] = make_float4(clo[1].z, chi[1].x, chi[1].y, chi[1].z);
     rec[4 * (size_t)i + 3] = make_float4(__int_as_float(cref[0]), __int_as_float(cref[1]), clo[0].w, clo[1].w);
-    float4 rlo, rhi;
-    node_region(keys, first[i], last[i], bits, morton, rlo, rhi);
-    reg[2 * (size_t)i] = rlo;
-    reg[2 * (size_t)i + 1] = rhi;
 }
 
 void lbvh_build(const Workspace &ws, int64_t n, int num_clouds, const float *points, const float *weights,
@@ -510,8 +453,8 @@ void lbvh_build(const Workspace &ws, int64_t n, int num_clouds, const float *poi
         k_refit<<<g, 256, 0, st>>>(ws.pts, n, ws.left, ws.right, ws.parent_int, ws.parent_leaf, ws.flags, ws.nbox);
         ++g_launches;
         cudaMemsetAsync(ws.rparent, 0xFF, sizeof(int) * (size_t)n, st); // -1: no parent record
-        k_records<<<g, 256, 0, st>>>(ws.pts, n, ws.left, ws.right, ws.first, ws.last, ws.nbox, ka, bits, ws.morton,
-                                     leaf_size, ws.records, ws.region, ws.rparent, ws.pleaf);
+        k_records<<<g, 256, 0, st>>>(ws.pts, n, ws.left, ws.right, ws.first, ws.nbox, leaf_size, ws.records,
+                                     ws.rparent, ws.pleaf);
     }
     ++g_launches;
     k_cloud_roots<<<(num_clouds + 127) / 128, 128, 0, st>>>(ws.cloud_off, num_clouds, leaf_size, ws.first, ws.last,
