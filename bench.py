@@ -15,7 +15,9 @@ region.
 
 Workloads: clustered_voronoi_5m (default), clustered_voronoi_500k,
 uniform_voronoi_100k, uniform_power_1m, lattice_power_310 (29.8M-point jittered
-lattice, power), surface_batch_256 (256 surface clouds in one CUDA-graph batch).
+lattice, power: learned radius + batched CUDA-graph build, plain beside it;
+``--plain`` for the single-cloud plain build), surface_batch_256 (256 surface
+clouds in one CUDA-graph batch).
 
 For N > 1 (torch.distributed.run, one process per GPU) every rank builds its
 own diagram of an equally sized, differently seeded point set (weak scaling;
@@ -337,6 +339,48 @@ def run_reference(args, spec, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def vertex_error(pts, w, count, rel, bound, planes, cells) -> dict:
+    """Exported vertex positions of `cells` against their FP64 positions.
+
+    Each vertex is the intersection of three planes; relative to its cell's point s the bisector
+    with q is (q - s) . x = (|q - s|^2 - (w_q - w_s)) / 2 and a face of the reference's FP32 box
+    (voronoi_ultra.cu:234-238) is x_axis = b - s_axis. The 3x3 systems are solved in FP64 from
+    the FP32 inputs. Reported: max and median of |x - x64| / |x64|, the max absolute error, and
+    how many vertices lie farther than their exported bound.
+    """
+    p = pts.astype(np.float64)
+    wt = np.zeros(len(p)) if w is None else w.astype(np.float64)
+    f = np.float32
+    lo = ((pts.min(0) - f(1.0)).astype(f) - f(1e-5)).astype(np.float64)
+    hi = ((pts.max(0) + f(1.0)).astype(f) + f(1e-5)).astype(np.float64)
+    k = np.minimum(count[cells], rel.shape[1])
+    cell = np.repeat(cells, k)
+    slot = np.concatenate([np.arange(x) for x in k])
+    x = rel[cell, slot].astype(np.float64)
+    b = bound[cell, slot].astype(np.float64)
+    pl = planes[cell, slot].astype(np.int64)
+    s = p[cell]
+    A = np.zeros((len(cell), 3, 3))
+    rhs = np.zeros((len(cell), 3))
+    for e in range(3):
+        ids = pl[:, e]
+        bis = ids >= 0
+        q = np.where(bis, ids, 0)
+        a = p[q] - s
+        code = -1 - ids
+        axis = np.where(bis, 0, code >> 1)
+        A[:, e, :] = np.where(bis[:, None], a, np.eye(3)[axis])
+        face = np.where(code & 1, hi[axis], lo[axis]) - s[np.arange(len(cell)), axis]
+        rhs[:, e] = np.where(bis, 0.5 * ((a * a).sum(1) - (wt[q] - wt[cell])), face)
+    x64 = np.linalg.solve(A, rhs[..., None])[..., 0]
+    err = np.linalg.norm(x - x64, axis=1)
+    rel_err = err / np.maximum(np.linalg.norm(x64, axis=1), 1e-300)
+    return {"vertices": int(err.size), "cells": int(len(cells)), "max_rel": float(rel_err.max()),
+            "median_rel": float(np.median(rel_err)), "max_abs": float(err.max()),
+            "beyond_bound": int((err > b + 1e-12 * np.linalg.norm(x64, axis=1)).sum()),
+            "reference": "FP64 solve of each vertex's three planes from the FP32 inputs"}
+
+
 def _timed(fn, steps, dev, flush):
     """Run fn `steps` times, L2 flushed before each, timed with CUDA events on the current stream."""
     import torch
@@ -435,6 +479,8 @@ def run_gpu(args, spec, rank, world, local):
     torch.cuda.set_device(dev)
     if spec["kind"] == "surfaces":
         return run_batch_gpu(args, spec, rank, world, local, dev)
+    if spec["kind"] == "lattice" and not args.plain:
+        return run_lattice_gpu(args, spec, rank, world, local, dev)
     pts, w = make_points(spec, seed=rank)
     n = pts.shape[0]
     h_pts = torch.from_numpy(pts).pin_memory()
@@ -452,14 +498,20 @@ def run_gpu(args, spec, rank, world, local):
         return pc._run(d_pts, d_w, 8, False, None, None, -1, profile=profile,
                        model=blob if with_model else None)
 
+    phases = {}
+
     def cell_pass_ms(with_model=True):
         # phase times come from a separate profiled build: the timed steps carry no per-phase events
-        ms = []
+        ms, prs = [], []
         for _ in range(3):
             flush.fill_(1.0)
             step_device(with_model, profile=True)
             pr = pc.last_profile()
+            prs.append(pr)
             ms.append(pr["cells_ms"] + pr["deferred_ms"])  # both cell launches
+        if with_model or not use_model:
+            phases.update({k: round(statistics.median(p[k] for p in prs), 3)
+                           for k in ("lbvh_ms", "cells_ms", "deferred_ms", "csr_ms")})
         return statistics.median(ms)
 
     host_out = _PinnedOut()
@@ -525,6 +577,15 @@ def run_gpu(args, spec, rank, world, local):
                      "cells_with_other_degree_or_status": int((dd | (fs != st)).sum())}
     cells_main = cell_pass_ms(True)
     cells_plain = cell_pass_ms(False) if use_model else None
+    vtx_err = None
+    if rank == 0:
+        # the position error of the builder's vertices, on the first 200k cells of one more build
+        _, vst = pc.build_with_stats(d_pts, d_w, vertices=64)
+        m = min(n, 200_000)
+        vtx_err = vertex_error(pts[: n], w, vst["vertex_count"].cpu().numpy(), vst["vertices"][:m].cpu().numpy(),
+                               vst["vertex_bound"][:m].cpu().numpy(), vst["vertex_planes"][:m].cpu().numpy(),
+                               np.arange(m))
+        del vst
 
     if rank == 0:
         off_np = off.cpu().numpy()
@@ -538,9 +599,13 @@ def run_gpu(args, spec, rank, world, local):
                   "escalation": {"fp32_tests_per_cell": cnt["tests"] / n,
                                  "fp64_fraction": cnt["fp64_escalations"] / max(cnt["tests"], 1),
                                  "exact_fraction": cnt["exact_escalations"] / max(cnt["tests"], 1),
-                                 "fp64_vertices_per_cell": cnt["vertex64"] / n},
+                                 "fp64_vertices_per_cell": cnt["vertex64"] / n,
+                                 "vertex_error": vtx_err},
                   "work_per_cell": {k: round(cnt[k] / n, 3) for k in ("nodes", "leaves", "candidates", "clips",
-                                                                       "deferred_cells")}}
+                                                                       "deferred_cells")},
+                  "phases_ms": dict(phases, note="one profiled build: LBVH (+ prediction), first cell pass, "
+                                                 "deferred-cell pass, CSR count + scan; the CSR fill runs in "
+                                                 "the adjacency emission")}
         if fp32_only is not None:
             config["fp32_only_predicates"] = fp32_only
         if use_model:
@@ -572,6 +637,104 @@ def run_gpu(args, spec, rank, world, local):
             "cpu_baseline": _cpu_baseline(args, world, pts, w, n),
             "clocks": csum,
             "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_lattice_gpu(args, spec, rank, world, local, dev):
+    """The jittered 310^3 power lattice as its configuration states it: learned search radius (a model
+    trained before timing on two 100^3 jittered lattices of other seeds), FP32-filtered predicates
+    with FP64 / exact escalation, and the batched path (one cloud, CUDA-graph replay), unchunked;
+    the plain batched build is timed beside it."""
+    import torch
+
+    import paragram_b200.cuda as pc
+    from paragram_b200 import dist, learned
+    from paragram_b200 import workloads as W
+    from paragram_b200.batch import build_batch
+
+    pts, w = make_points(spec, seed=rank)
+    n = pts.shape[0]
+    h_pts, h_w = torch.from_numpy(pts).pin_memory(), torch.from_numpy(w).pin_memory()
+    d_pts, d_w = h_pts.to(dev), h_w.to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    t0 = time.perf_counter()
+    data = [learned.collect(*[torch.from_numpy(a).to(dev) for a in W.jittered_lattice(100, seed=1000 + 2 * rank + k)])
+            for k in range(2)]
+    log = []
+    model = learned.train(data, epochs=4, batch=8192, log=log)
+    margin = model.calibrate(data[0], quantile=0.98)
+    del data
+    torch.cuda.synchronize(dev)
+    train_info = {"train_s": time.perf_counter() - t0, "loss_per_epoch": [round(x, 4) for x in log],
+                  "margin": margin, "calibration_quantile": 0.98, "trained_on": "two 100^3 jittered lattices"}
+
+    def step(with_model=True):
+        return build_batch([d_pts], [d_w], graph=True, model=model if with_model else None)
+
+    host_out = _PinnedOut()
+
+    def step_e2e():
+        d = build_batch([h_pts.to(dev, non_blocking=True)], [h_w.to(dev, non_blocking=True)], graph=True,
+                        model=model)[0]
+        return host_out.copy("a", d.adjacency), host_out.copy("o", d.offsets), host_out.copy("s", d.status)
+
+    for _ in range(args.warmup):
+        step()
+        step(False)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    times, plain_times = [], []
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            t, _, _, out = _timed(step, 1, dev, flush)
+            times += t
+            t, _, _, _ = _timed(lambda: step(False), 1, dev, flush)
+            plain_times += t
+    dist.barrier()
+    total_cells = dist.reduce_sum(float(n) * args.steps, dev)
+    value = total_cells / (dist.reduce_max(sum(times), dev) / 1e3) / 1e6
+    plain_value = total_cells / (dist.reduce_max(sum(plain_times), dev) / 1e3) / 1e6
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    e2e_times, _, _, (a, o, s) = _timed(step_e2e, args.steps, dev, flush)
+    e2e_value = total_cells / (dist.reduce_max(sum(e2e_times), dev) / 1e3) / 1e6
+    d2h = a.numel() * 4 + o.numel() * 4 + s.numel() * 4
+    # counters and phase times of the same build through the single-cloud entry point (untimed)
+    _, cnt = pc.build_with_stats(d_pts, d_w, model=model.blob, profile=True)
+    prof = pc.last_profile()
+    if rank == 0:
+        d = out[0]
+        off_np = d.offsets.cpu().numpy()
+        flops, nbytes = algorithmic_work(off_np, True)
+        cell_s = (prof["cells_ms"] + prof["deferred_ms"]) / 1e3
+        csum = clocks.summary()
+        line = {
+            "metric": "Mcells/s", "value": value, "unit": "Mcells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": statistics.mean(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "step_ms": [round(t, 2) for t in times],
+            "config": {"workload": args.workload, "n_points": n, "weighted": True,
+                       "l2": "flushed between steps (256 MiB write)", "launch": "batched build, CUDA graph replay",
+                       "chunks": int(prof["chunks"]), "parallelism": f"independent diagram per GPU x{world}",
+                       "predicates": "FP32 filtered, FP64 / exact escalation",
+                       "escalation": {"fp32_tests_per_cell": cnt["tests"] / n,
+                                      "fp64_fraction": cnt["fp64_escalations"] / max(cnt["tests"], 1),
+                                      "exact_fraction": cnt["exact_escalations"] / max(cnt["tests"], 1),
+                                      "fp64_vertices_per_cell": cnt["vertex64"] / n},
+                       "search_radius": "learned (MLP 16-64-64-2, BF16, trained before timing)",
+                       "learned": dict(train_info, fallback_rate=cnt["hint_misses"] / n,
+                                       hit_rate=cnt["hint_hits"] / n),
+                       "plain": {"value": plain_value, "unit": "Mcells/s",
+                                 "ms_per_step": statistics.mean(plain_times)},
+                       "learned_over_plain": value / plain_value,
+                       "status_counts": np.bincount(d.status.cpu().numpy(), minlength=6)[:6].tolist(),
+                       "phases_ms": {k: round(prof[k], 3) for k in ("lbvh_ms", "cells_ms", "deferred_ms", "csr_ms")}},
+            "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": n * 16, "d2h_bytes_per_step": d2h},
+            "roofline": _roofline(flops, nbytes, cell_s, csum, "k_cells_fast (cell pass)", None),
+            "cpu_baseline": _cpu_baseline(args, world, pts, w, n),
+            "clocks": csum,
+            "gpu_launches": int(prof["launches"]) * args.steps,
         }
         print(json.dumps(line), flush=True)
 

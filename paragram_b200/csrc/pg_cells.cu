@@ -87,6 +87,8 @@ template <int CAP, int STACK> struct CellMem
     float skey[STACK]; // lower bound of the bisector distance of any point of the pending node
     unsigned long long cnt[kNumStats]; // per-warp statistics (written by lane 0)
     unsigned long long cnt0[3];        // nodes, leaves, candidates at the start of the current cell
+    float cap;  // search radius of the current pass (learned / given; +inf without one)
+    float done; // search radius of the finished first pass (-inf during the first pass)
     unsigned et[CAP * CAP / 32];       // edge table of the clip in progress (all zero between clips)
 };
 
@@ -752,24 +754,38 @@ __device__ __forceinline__ int clip(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, 
     return kClipChanged;
 }
 
-template <int CAP, int STACK> __device__ __forceinline__ void update_rsafe(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int lane)
+// Radius of the current cell: no vertex lies farther from the seed (with its error bound).
+template <int CAP, int STACK> __device__ __forceinline__ float cell_radius(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int lane)
 {
     float mx = 0.0f;
 #pragma unroll(CAP > 256 ? 1 : CAP / 32)
     for (int k = 0; k < CAP / 32; ++k)
         if ((ws.valid[k] >> lane) & 1u)
             mx = fmaxf(mx, m.vr[k * 32 + lane]);
-    ws.rsafe = sqrtf(__uint_as_float(__reduce_max_sync(kFull, __float_as_uint(mx)))) * (1.0f + 1e-6f);
+    return sqrtf(__uint_as_float(__reduce_max_sync(kFull, __float_as_uint(mx)))) * (1.0f + 1e-6f);
+}
+
+// The pruning radius: the cell's radius, capped by the pass's search radius (HINT)
+template <int CAP, int STACK, bool HINT>
+__device__ __forceinline__ void update_rsafe(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int lane)
+{
+    float r = cell_radius(m, ws, lane);
+    ws.rsafe = HINT ? fminf(r, m.cap) : r;
 }
 
 // Process one batch of candidates (one per lane, `have` marks real ones).
 // Returns false when the cell is finished early (empty or deferred).
-template <int CAP, int STACK>
+template <int CAP, int STACK, bool HINT>
 __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, bool have, const Cand &q, float key,
-                                          const CellArgs &A, int lane, VMask<CAP / 32> vmask, bool masked)
+                                          const CellArgs &A, int lane, VMask<CAP / 32> vmask, bool masked,
+                                          bool old_leaf = false)
 {
-    // security radius: no vertex can be removed when h - eh > |a| * rsafe
+    // security radius: no vertex can be removed when h - eh > |a| * rsafe (the pruning radius)
     if (have && (q.h - q.eh) > q.nrm * ws.rsafe * (1.0f + 1e-6f))
+        have = false;
+    // second pass of a capped cell: in a leaf the first pass visited, the candidates within
+    // the first pass's radius were clipped then (or could not clip: the cell only shrinks)
+    if (HINT && old_leaf && have && !((q.h - q.eh) > q.nrm * m.done * (1.0f + 1e-6f)))
         have = false;
     unsigned hv = __ballot_sync(kFull, have);
     if (hv == 0u)
@@ -818,7 +834,7 @@ __device__ __forceinline__ bool run_batch(CellMem<CAP, STACK> &m, WarpState<CAP>
         changed = changed || r == kClipChanged;
     }
     if (changed)
-        update_rsafe(m, ws, lane);
+        update_rsafe<CAP, STACK, HINT>(m, ws, lane);
     return true;
 }
 
@@ -990,9 +1006,9 @@ __device__ __forceinline__ bool write_outputs(CellMem<CAP, STACK> &m, WarpState<
 }
 
 // One BVH leaf as a candidate batch (one point per lane).
-template <int CAP, int STACK, bool GUESS>
+template <int CAP, int STACK, bool GUESS, bool HINT>
 __device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int ref, int i,
-                                           const CellArgs &A, int lane, VMask<CAP / 32> vm)
+                                           const CellArgs &A, int lane, VMask<CAP / 32> vm, bool old_leaf)
 {
     PG_COUNT(m, lane, kStatLeaves, 1);
     int first = leaf_first(ref), count = leaf_count(ref);
@@ -1010,20 +1026,18 @@ __device__ __forceinline__ bool leaf_batch(CellMem<CAP, STACK> &m, WarpState<CAP
             for (int t = 0; t < ws.np && have; ++t)
                 have = m.pid[t] != j;
     }
-    return run_batch(m, ws, have, q, qkey, A, lane, vm, true);
+    return run_batch<CAP, STACK, HINT>(m, ws, have, q, qkey, A, lane, vm, true, old_leaf);
 }
 
 // Best-first BVH traversal of one cell. A pending entry is (parent << 1 | side)
 // with a lower bound of the bisector distance of the child's points; the
 // entry with the smallest bound is popped, dropped if the bound exceeds the
-// radius of the (since shrunk) cell or `cap`, else its box is tested against
-// every vertex's empty sphere and, for a leaf, only the vertices that pass are
-// pre-tested. `capped` reports whether the cap alone dropped a node; leaves
-// whose bound is <= done_cap are skipped (clipped by an earlier pass). Returns
-// false when the cell finished early (emptied or deferred).
+// pruning radius (the radius of the since shrunk cell; with a search radius,
+// at most that), else its box is tested against every vertex's empty sphere
+// and, for a leaf, only the vertices that pass are pre-tested. Returns false
+// when the cell finished early (emptied or deferred).
 template <int CAP, int STACK, bool GUESS, bool HINT>
-__device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int i, const CellArgs &A, int lane,
-                                         float cap, float done_cap, bool &capped)
+__device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> &ws, int i, const CellArgs &A, int lane)
 {
     const float4 *rec = A.rec;
     // Start at the seed's own leaf (bound 0) and queue the sibling of every node
@@ -1060,11 +1074,6 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
             float k;
             bool p = side == 1 ? box_key(ws, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r3.z, k)
                                : box_key(ws, r1.z, r1.w, r2.x, r2.y, r2.z, r2.w, r3.w, k);
-            if (HINT)
-            {
-                capped = capped || (p && k > cap);
-                p = p && !(k > cap);
-            }
             if (p)
             {
                 if (lane == 0)
@@ -1114,13 +1123,6 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
                 break; // every pending bound exceeds the radius: the cell is final
             continue;
         }
-        if (HINT && key > cap)
-        {
-            capped = true;
-            if (floor_key > cap)
-                break;
-            continue;
-        }
         PG_COUNT(m, lane, kStatNodes, 1);
         float lx, ly, lz, hx, hy, hz, mw;
         int ref;
@@ -1148,8 +1150,6 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
                 ref = __float_as_int(r3.y);
             }
         }
-        if (HINT && ref_is_leaf(ref) && !(key > done_cap))
-            continue; // clipped by the first pass
         VMask<CAP / 32> vm;
         bool any = node_vertex_mask(m, ws, lx, ly, lz, hx, hy, hz, mw, lane, vm);
         PG_T1(m, lane, kStatCycNodes, tn);
@@ -1158,7 +1158,7 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
         if (ref_is_leaf(ref))
         {
             PG_T0(tl);
-            bool go = leaf_batch<CAP, STACK, GUESS>(m, ws, ref, i, A, lane, vm);
+            bool go = leaf_batch<CAP, STACK, GUESS, HINT>(m, ws, ref, i, A, lane, vm, HINT && !(key > m.done));
             PG_T1(m, lane, kStatCycLeaves, tl);
             if (!go)
                 return false;
@@ -1171,12 +1171,6 @@ __device__ __forceinline__ bool traverse(CellMem<CAP, STACK> &m, WarpState<CAP> 
         float k0, k1;
         bool p0 = box_key(ws, c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c3.z, k0);
         bool p1 = box_key(ws, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w, c3.w, k1);
-        if (HINT)
-        {
-            capped = capped || (p0 && k0 > cap) || (p1 && k1 > cap);
-            p0 = p0 && !(k0 > cap);
-            p1 = p1 && !(k1 > cap);
-        }
         if (sp + 2 > STACK)
         {
             ws.flags |= kFlagDefer;
@@ -1254,38 +1248,57 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
             unsigned peers = __match_any_sync(kFull, have ? j : -2 - lane);
             if (have && (__ffs(peers) - 1) != lane)
                 have = false;
-            if (!run_batch(m, ws, have, q, key, A, lane, VMask<CAP / 32>{}, false))
+            if (!run_batch<CAP, STACK, false>(m, ws, have, q, key, A, lane, VMask<CAP / 32>{}, false))
                 return;
         }
     }
     PG_T1(m, lane, kStatCycWarm, tw);
-    // 2. BVH traversal, best first (traverse). With a search radius (learned or
-    // given), the first pass also drops every node whose bound exceeds it; if
-    // the final radius of the cell is within it, the dropped nodes could not
-    // clip the cell (certificate), else a second, unbounded pass follows and
-    // skips the leaves already clipped.
-    float cap = INFINITY, done_cap = -1.0f;
-    if (HINT && A.hint != nullptr)
+    // 2. BVH traversal, best first (traverse). With a search radius R (learned or
+    // given), the first pass prunes nodes and candidates at min(cell radius, R):
+    // whatever lies beyond R cannot cut a cell whose radius is within R, so the
+    // pass is certified when the final cell's radius is <= R (and it skips the
+    // transient clips by points beyond R). Otherwise a second pass completes the
+    // cell without the cap; in the leaves the first pass visited it takes only
+    // the candidates beyond R.
+    if (!HINT)
+    {
+        traverse<CAP, STACK, GUESS, false>(m, ws, i, A, lane);
+        return;
+    }
+    float cap = INFINITY;
+    if (A.hint != nullptr)
     {
         float rq = A.hint[i];
         if (rq > 0.0f && rq < 1e30f)
             cap = rq;
     }
-    for (int pass = 0; pass < 2; ++pass)
+    if (lane == 0)
     {
-        bool capped = false;
-        if (!traverse<CAP, STACK, GUESS, HINT>(m, ws, i, A, lane, cap, done_cap, capped))
+        m.cap = cap;
+        m.done = -INFINITY;
+    }
+    __syncwarp();
+    ws.rsafe = fminf(ws.rsafe, cap);
+    for (int pass = 0;; ++pass) // one inlined copy of the traversal for both passes
+    {
+        if (!traverse<CAP, STACK, GUESS, true>(m, ws, i, A, lane))
             return;
-        if (!HINT || !capped)
+        float r = cell_radius(m, ws, lane);
+        ws.rsafe = r;
+        if (pass == 1 || cap == INFINITY)
             return;
-        if (ws.rsafe <= cap)
+        if (r <= cap)
         {
             PG_COUNT(m, lane, kStatHintHit, 1);
             return;
         }
         PG_COUNT(m, lane, kStatHintMiss, 1);
-        done_cap = cap;
-        cap = INFINITY;
+        if (lane == 0)
+        {
+            m.cap = INFINITY;
+            m.done = cap;
+        }
+        __syncwarp();
     }
 }
 
