@@ -616,6 +616,8 @@ def run_gpu(args, spec, rank, world, local):
                                "step_ms": [round(t, 2) for t in plain[0]],
                                "cell_pass_ms": cells_plain}
             config["learned_over_plain"] = value / plain_value if plain_value else None
+            # the same ratio from the median step times (robust to an occasional slow step)
+            config["learned_over_plain_median"] = statistics.median(plain[0]) / statistics.median(times)
         line = {
             "metric": "Mcells/s",
             "value": value,
@@ -728,6 +730,7 @@ def run_lattice_gpu(args, spec, rank, world, local, dev):
                        "plain": {"value": plain_value, "unit": "Mcells/s",
                                  "ms_per_step": statistics.mean(plain_times)},
                        "learned_over_plain": value / plain_value,
+                       "learned_over_plain_median": statistics.median(plain_times) / statistics.median(times),
                        "status_counts": np.bincount(d.status.cpu().numpy(), minlength=6)[:6].tolist(),
                        "phases_ms": {k: round(prof[k], 3) for k in ("lbvh_ms", "cells_ms", "deferred_ms", "csr_ms")}},
             "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": n * 16, "d2h_bytes_per_step": d2h},

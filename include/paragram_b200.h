@@ -220,6 +220,17 @@ int pg_mlp_adam(float *params, const float *grad, float *m, float *v, int64_t st
                 float beta2, float eps, void *model, void *stream);
 int pg_mlp_pack(const float *params, void *model, void *stream);
 
+/* Facet areas of a built diagram, aligned with its adjacency (no reference counterpart: the
+ * reference computes each cell's polytope and keeps only the neighbour ids, voronoi_ultra.cu:125-138).
+ * Inputs are the vertex export of the build (pg_options.vertices_out, vertex_planes_out,
+ * vertex_count_out with capacity vertex_cap <= 256), the build's points (float32 [N * 3]) and its
+ * Diagram (offsets [N + 1], adjacency [E]). areas (float32 [E], output): for entry e of row u, the
+ * area of the facet between u's cell and adjacency[e]'s; NaN when a cell's vertices exceeded
+ * vertex_cap. All pointers are device pointers; ordered on stream. */
+int pg_face_areas(int64_t num_points, int32_t vertex_cap, const float *vertices, const int32_t *vertex_planes,
+                  const int32_t *vertex_count, const float *points, const int32_t *offsets, const int32_t *adjacency,
+                  float *areas, void *stream);
+
 /* CSR offsets from per-row degrees, allocating nothing. No counterpart in the
  * reference: it is for callers that cannot allocate device memory when they
  * call (a device-memory budget fixed at start-up, device memory owned by

@@ -8,13 +8,14 @@ fallback -- calling the API without the built library raises ImportError.
 
 from ._api import Diagram, power_diagram, voronoi_diagram
 from .batch import build_batch
-from .geometry import cell_geometry, cell_vertices
+from .geometry import cell_geometry, cell_vertices, face_areas
 
 __all__ = [
     "Diagram",
     "build_batch",
     "cell_geometry",
     "cell_vertices",
+    "face_areas",
     "power_diagram",
     "voronoi_diagram",
 ]

@@ -41,7 +41,7 @@ class PgOptions(ctypes.Structure):
 EXPORTED = ["pg_version", "pg_last_error", "pg_workspace_size", "pg_build", "pg_emit_adjacency", "pg_stats",
             "pg_last_profile", "pg_degrees_to_offsets_noalloc", "pg_batch_workspace_size", "pg_build_batch",
             "pg_batch_check", "pg_mlp_num_params", "pg_mlp_model_bytes", "pg_mlp_forward", "pg_mlp_grad",
-            "pg_mlp_adam", "pg_mlp_pack"]
+            "pg_mlp_adam", "pg_mlp_pack", "pg_face_areas"]
 
 
 def load() -> ctypes.CDLL:
@@ -88,6 +88,8 @@ def load() -> ctypes.CDLL:
         lib.pg_mlp_adam.restype = ctypes.c_int
         lib.pg_mlp_pack.argtypes = [vp, vp, vp]
         lib.pg_mlp_pack.restype = ctypes.c_int
+        lib.pg_face_areas.argtypes = [i64, i32, vp, vp, vp, vp, vp, vp, vp, vp]
+        lib.pg_face_areas.restype = ctypes.c_int
         lib.pg_degrees_to_offsets_noalloc.argtypes = [i64, vp, vp, vp]
         lib.pg_degrees_to_offsets_noalloc.restype = ctypes.c_int
         _lib = lib

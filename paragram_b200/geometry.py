@@ -61,4 +61,32 @@ def cell_vertices(points: torch.Tensor, weights: Optional[torch.Tensor] = None, 
     return Diagram(adjacency=adjacency, offsets=offsets, status=status), verts
 
 
-__all__ = ["cell_geometry", "cell_vertices"]
+def face_areas(points: torch.Tensor, weights: Optional[torch.Tensor] = None, *, capacity: int = 64,
+               knn: int = 8, leaf_size: int = -1) -> Tuple[Diagram, torch.Tensor]:
+    """Build the diagram and return ``(diagram, areas)``: float32 [E], the area of the facet between
+    row u and each of its neighbours, aligned with ``diagram.adjacency`` (the transport and
+    finite-volume coefficients of a power diagram). Computed from the cells' exported vertices;
+    NaN for a cell with more than ``capacity`` vertices (at most 256).
+    """
+    from . import _lib
+
+    d, vx = cell_vertices(points, weights, capacity=capacity, knn=knn, leaf_size=leaf_size)
+    points = _validate_points(points)
+    n = int(points.shape[0])
+    areas = torch.empty(max(d.adjacency.numel(), 1), dtype=torch.float32, device=points.device)
+    if n > 0 and d.adjacency.numel() > 0:
+        lib = _lib.load()
+        rel = vx["relative"]
+        # the library reads the exported float4 rows (x, y, z, bound)
+        v4 = torch.cat([rel, vx["bound"][..., None]], dim=2).contiguous()
+        with torch.cuda.device(points.device):
+            rc = lib.pg_face_areas(n, int(capacity), v4.data_ptr(), vx["planes"].contiguous().data_ptr(),
+                                   vx["count"].contiguous().data_ptr(), points.data_ptr(), d.offsets.data_ptr(),
+                                   d.adjacency.data_ptr(), areas.data_ptr(),
+                                   torch.cuda.current_stream(points.device).cuda_stream)
+        if rc != 0:
+            raise RuntimeError(_lib.last_error(lib))
+    return d, areas[: d.adjacency.numel()]
+
+
+__all__ = ["cell_geometry", "cell_vertices", "face_areas"]
