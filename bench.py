@@ -783,6 +783,9 @@ def run_batch_gpu(args, spec, rank, world, local, dev):
     e2e_times, _, _, res = _timed(step_e2e, args.steps, dev, flush)
     e2e_value = total_cells / (dist.reduce_max(sum(e2e_times), dev) / 1e3) / 1e6
     d2h = sum(a.numel() * 4 + o.numel() * 4 + s.numel() * 4 for a, o, s in res)
+    # phase times of one more (untimed, not captured) build of the same batch
+    build_batch(d_clouds, graph=False, profile=True)
+    prof = pc.last_profile()
     if rank == 0:
         flops = nbytes = 0.0
         status = np.zeros(6, np.int64)
@@ -800,7 +803,9 @@ def run_batch_gpu(args, spec, rank, world, local, dev):
             "config": {"workload": args.workload, "clouds": len(clouds), "n_points": n,
                        "cloud_sizes": [int(min(len(c) for c in clouds)), int(max(len(c) for c in clouds))],
                        "l2": "flushed between steps (256 MiB write)", "launch": "one CUDA graph per batch shape",
-                       "status_counts": status.tolist(), "parallelism": f"independent batch per GPU x{world}"},
+                       "status_counts": status.tolist(), "parallelism": f"independent batch per GPU x{world}",
+                       "phases_ms": {k: round(prof[k], 3) for k in ("lbvh_ms", "cells_ms", "deferred_ms", "csr_ms",
+                                                                     "deferred_cells")}},
             "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": n * 12, "d2h_bytes_per_step": d2h},
             "roofline": _roofline(flops, nbytes, step_s, csum, "whole batched build (graph replay)", None),
             "cpu_baseline": _cpu_baseline_clouds(args, world, clouds),

@@ -169,7 +169,7 @@ int pg_emit_adjacency(int64_t num_points, const void *workspace, const int32_t *
 
 /* Counters of the last pg_build on this workspace (synchronises the stream):
  * out[0] FP32 side tests, out[1] tests escalated to FP64, out[2] tests escalated
- * to exact expansions, out[3] cells deferred to the 256-slot pass, out[4] BVH
+ * to exact expansions, out[3] deferrals to a larger tier (128 slots, then 256), out[4] BVH
  * nodes visited, out[5] leaves visited, out[6] clips that changed a cell,
  * out[7] candidates that reached the vertex test. No reference counterpart
  * (the reference only prints timings, voronoi_ultra.cu:196-219). */

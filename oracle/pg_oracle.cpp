@@ -32,7 +32,7 @@
 // i < j (original point index), which makes the result independent of the
 // order in which candidates are clipped.
 //
-// Deliberate differences from the reference (documented in DESIGN.md):
+// Deliberate differences from the reference:
 //   * the power "too far" test of faster_convex_cell.cuh:391-408 uses |t|,
 //     which skips planes lying behind the seed; here such planes clip (the
 //     cell becomes empty, as in the exact power diagram);

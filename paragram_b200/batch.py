@@ -64,13 +64,15 @@ class _Static:
 
 def build_batch(points: Sequence[torch.Tensor], weights: Optional[Sequence[torch.Tensor]] = None, *,
                 leaf_size: int = -1, graph: bool = False, blocks_per_sm: int = 0, model=None,
-                geometry_out: Optional[torch.Tensor] = None) -> list[Diagram]:
+                geometry_out: Optional[torch.Tensor] = None, profile: bool = False) -> list[Diagram]:
     """Diagrams of independent clouds (Voronoi, or power when ``weights`` is given) in one build.
 
     ``model``: a trained ``paragram_b200.learned.Model`` (its search radius per point, predicted for
     every cloud in the same launch); the diagrams do not depend on it. ``geometry_out``: a float32
     [total points, 4] CUDA tensor (clouds concatenated in order) that receives each cell's
     centroid (x, y, z) and volume, as ``paragram_b200.cell_geometry`` does for one cloud.
+    ``profile=True`` (not with ``graph``) records the phase times that
+    ``paragram_b200.cuda.last_profile()`` returns.
     """
     if len(points) == 0:
         return []
@@ -102,7 +104,9 @@ def build_batch(points: Sequence[torch.Tensor], weights: Optional[Sequence[torch
     key = (dev.index, tuple(int(p.shape[0]) for p in points), weights is not None, int(leaf_size),
            int(blocks_per_sm), None if blob is None else blob.data_ptr(),
            None if geometry_out is None else geometry_out.data_ptr())
-    opts = _lib.PgOptions(8, int(leaf_size), 0, 0, int(blocks_per_sm))
+    if profile and graph:
+        raise ValueError("profile=True records host-side phase times and cannot be captured in a graph")
+    opts = _lib.PgOptions(8, int(leaf_size), 2 if profile else 0, 0, int(blocks_per_sm))
     if blob is not None:
         opts.model = blob.data_ptr()
     if geometry_out is not None and total_points > 0:

@@ -79,6 +79,8 @@ size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
     w.rows = (int *)take(4 * N * kRowWidth);
     w.deg = (int *)take(4 * N);
     w.big_list = (int *)take(4 * N);
+    w.big_list2 = (int *)take(4 * (size_t)big_cap((int64_t)N));
+    w.big_slot2 = (int *)take(4 * (size_t)big_cap((int64_t)N));
     w.big_rows = (int *)take(4 * (size_t)big_cap((int64_t)N) * kBigRowWidth);
     w.big_slabs = take(big_slab_bytes());
     w.huge_slabs = take(huge_slab_bytes());

@@ -32,9 +32,10 @@
 // tested lane-parallel over the vertices.
 //
 // A cell that needs more than 64 vertex / plane slots is deferred to a second
-// launch with 256 slots in global memory (then 512 if needed); its status is
-// then vertex_overflow (2) if the final cell has more than 64 vertices (the
-// reference MAX_VERTS) and plane_overflow (1) only if even 512 slots overflow.
+// launch with 128 slots in shared memory, then to a third with 256 slots in
+// global memory (then 512 if needed); its status is then vertex_overflow (2)
+// if the final cell has more than 64 vertices (the reference MAX_VERTS) and
+// plane_overflow (1) only if even 512 slots overflow.
 //
 // With a geometry output, each final cell is also integrated before it is
 // discarded (integrate_cell: volume and centroid from a fan of signed
@@ -118,6 +119,8 @@ struct CellArgs
     int *deg;
     int *status;
     int *big_list;
+    int *big_list2;  // cells that outgrew the middle tier too, and their deferred-row slots
+    int *big_slot2;
     int *big_rows;
     int *counters;
     unsigned long long *stats;
@@ -1385,23 +1388,6 @@ __device__ __forceinline__ void integrate_cell(CellMem<CAP, STACK> &m, const Cel
                         succ[k][r] = j;
         }
     }
-    // The FP32 vertices are only as accurate as the side tests need (psi); rebuild in FP64 the
-    // ones whose bound exceeds 32 ulps of their size, so that each vertex is within about
-    // 2^-19 |v| of the exact one (a power cell far from its seed amplifies that by |v| / size).
-#pragma unroll(CAP > 256 ? 1 : CAP / 32)
-    for (int k = 0; k < W; ++k)
-        if ((valid[k] >> lane) & 1u)
-        {
-            int slot = k * 32 + lane;
-            float4 X = m.vx[slot];
-            if (!(X.w <= 32.0f * kEps * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z))))
-            {
-                unsigned t = m.vt[slot];
-                m.vx[slot] = vertex64_plain(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], A.pts,
-                                            A.oid, box, s, X);
-            }
-        }
-    __syncwarp();
     // apex: the mean vertex (inside the cell), not the seed, which a power cell may lie far from;
     // tetrahedra from a distant apex would cancel to the cell's small volume
     float ox = 0.0f, oy = 0.0f, oz = 0.0f, on = 0.0f;
@@ -1515,6 +1501,30 @@ __device__ __forceinline__ void write_vertices(CellMem<CAP, STACK> &m, const Cel
         A.vertex_count_out[soid] = base;
 }
 
+// The FP32 vertices are only as accurate as the side tests need (psi); before an
+// export, rebuild in FP64 the ones whose bound exceeds 32 ulps of their size, so
+// that each vertex is within about 2^-19 |v| of the exact one (a power cell far
+// from its seed amplifies that by |v| / size). psi stays a valid bound.
+template <int CAP, int STACK>
+__device__ __forceinline__ void refine_vertices(CellMem<CAP, STACK> &m, const CellArgs &A, int lane, float4 s,
+                                                const float *box)
+{
+    constexpr int W = WarpState<CAP>::W;
+    for (int k = 0; k < W; ++k)
+        if ((m.eb[k] >> lane) & 1u)
+        {
+            int slot = k * 32 + lane;
+            float4 X = m.vx[slot];
+            if (!(X.w <= 32.0f * kEps * (fabsf(X.x) + fabsf(X.y) + fabsf(X.z))))
+            {
+                unsigned t = m.vt[slot];
+                m.vx[slot] = vertex64_plain(m.pid[tri_get(t, 0)], m.pid[tri_get(t, 1)], m.pid[tri_get(t, 2)], A.pts,
+                                            A.oid, box, s, X);
+            }
+        }
+    __syncwarp();
+}
+
 // Geometry and vertex export of a final cell (valid-slot masks in m.eb). A cell
 // deferred to the larger pass writes NaN geometry and no vertices (that pass
 // writes them); an empty cell volume 0, a NaN centroid and no vertices.
@@ -1524,6 +1534,8 @@ template <int CAP, int STACK>
 __device__ __noinline__ void export_cell(CellMem<CAP, STACK> &m, const CellArgs &A, int lane, int soid, float4 s,
                                          const float *box, int flags)
 {
+    if (!(flags & (kFlagDefer | kFlagEmpty)))
+        refine_vertices(m, A, lane, s, box);
     if (A.geometry_out != nullptr)
     {
         if (flags & (kFlagDefer | kFlagEmpty))
@@ -1539,7 +1551,7 @@ __device__ __noinline__ void export_cell(CellMem<CAP, STACK> &m, const CellArgs 
     }
     if ((A.vertex_count_out != nullptr || A.vertices_out != nullptr || A.vertex_planes_out != nullptr) &&
         !(flags & kFlagDefer))
-        write_vertices(m, A, lane, soid); // after the integration, which may refine vertices in place
+        write_vertices(m, A, lane, soid);
 }
 
 template <int CAP, int STACK>
@@ -1611,8 +1623,12 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
     if (lane < kNumStats)
         m.cnt[lane] = 0;
     clear_edges(m, lane);
-    int64_t count = A.big_pass ? min((int64_t)A.counters[1], A.big_cap) : (A.end - A.begin);
-    int *ctr = A.big_pass ? &A.counters[3] : &A.counters[0];
+    // pass 0: the cell range of this launch; pass 1 (middle tier): the cells deferred by
+    // pass 0; pass 2 (large tier): the cells deferred by pass 1, with their row slots
+    const int pass = A.big_pass;
+    int64_t count = pass == 0 ? (A.end - A.begin)
+                              : min((int64_t)A.counters[pass == 1 ? 1 : 5], A.big_cap);
+    int *ctr = &A.counters[pass == 0 ? 0 : (pass == 1 ? 3 : 6)];
     for (;;)
     {
         int t = 0;
@@ -1621,24 +1637,24 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
         t = __shfl_sync(kFull, t, 0);
         if (t >= count)
             break;
-        int i = A.big_pass ? A.big_list[t] : (int)(A.begin + t);
+        int i = pass == 0 ? (int)(A.begin + t) : (pass == 1 ? A.big_list[t] : A.big_list2[t]);
         PG_T0(tcell);
         process_cell<CAP, STACK, GUESS, HINT>(m, ws, i, A, lane);
         write_diagnostics(m, ws, A, lane);
-        if (A.big_pass)
-            ws.si = t; // the deferred-row slot
+        if (pass)
+            ws.si = pass == 1 ? t : A.big_slot2[t]; // the deferred-row slot
         if (__any_sync(kFull, ws.flags & kFlagError)) // a flag may be set on any lane
         {
             if (lane == 0)
                 atomicExch(&A.counters[2], 1);
             ws.flags &= ~kFlagError;
         }
-        if (A.big_pass && (ws.flags & kFlagDefer) && ws.si < A.big_cap && huge_cell(A, i, lane, ws.si))
+        if (pass == 2 && (ws.flags & kFlagDefer) && ws.si < A.big_cap && huge_cell(A, i, lane, ws.si))
             continue; // outgrew the 256 slots too: rebuilt with 512
-        if (!(ws.flags & kFlagDefer) || A.big_pass)
+        if (!(ws.flags & kFlagDefer) || pass == 2)
         {
             PG_T0(to);
-            bool done = write_outputs(m, ws, A, lane, A.big_pass != 0);
+            bool done = write_outputs(m, ws, A, lane, pass != 0);
             PG_T1(m, lane, kStatCycOut, to);
             if (done)
             {
@@ -1647,13 +1663,22 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
             }
         }
         PG_COUNT(m, lane, kStatDeferred, 1);
-        // deferred: placeholder outputs (an empty row) until the large-capacity pass
+        // deferred: placeholder outputs (an empty row) until a larger tier rebuilds the cell
         if (lane == 0)
         {
             A.deg[ws.soid] = 0;
             A.status[ws.soid] = kPlaneOverflow;
-            int d = atomicAdd(&A.counters[1], 1);
-            A.big_list[d] = i;
+            if (pass == 0)
+            {
+                int d = atomicAdd(&A.counters[1], 1);
+                A.big_list[d] = i;
+            }
+            else
+            {
+                int d = atomicAdd(&A.counters[5], 1);
+                A.big_list2[d] = i;
+                A.big_slot2[d] = ws.si;
+            }
         }
     }
     flush_stats(m, A, lane);
@@ -1665,6 +1690,17 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) k_cells_fast(CellAr
     __shared__ CellMem<kCapFast, kStackFast> mem[kWarpsPerBlock];
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     cells_body<kCapFast, kStackFast, GUESS, HINT>(mem[w], A, lane);
+}
+
+// Middle tier: the cells that outgrew 64 slots, with 128 slots and a 512-entry
+// queue in shared memory (its own launch, so its larger shared-memory carve-out
+// does not shrink the first pass's L1).
+template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_cells_mid(CellArgs A)
+{
+    extern __shared__ __align__(16) unsigned char mid_smem[];
+    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto *m = reinterpret_cast<CellMem<kCapMid, kStackMid> *>(mid_smem) + w;
+    cells_body<kCapMid, kStackMid, GUESS, false>(*m, A, lane);
 }
 
 template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_cells_big(CellArgs A)
@@ -1698,6 +1734,8 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.deg = ws.deg;
     A.status = nullptr;
     A.big_list = ws.big_list;
+    A.big_list2 = ws.big_list2;
+    A.big_slot2 = ws.big_slot2;
     A.big_rows = ws.big_rows;
     A.counters = ws.counters;
     A.stats = ws.stats;
@@ -1751,13 +1789,26 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
     kern<<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(A);
 }
 
-// The deferred count stays on the device: a fixed grid reads it.
+// The deferred counts stay on the device: fixed grids read them. Pass 1 (middle
+// tier, shared memory) rebuilds the cells pass 0 deferred; pass 2 (global slabs)
+// the ones that outgrew it too.
 void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st)
 {
     CellArgs A = make_args(ws, cl);
     A.status = status;
-    A.big_pass = 1;
     A.big_cap = big_cap;
+    const size_t mid_smem = sizeof(CellMem<kCapMid, kStackMid>) * kWarpsPerBlock;
+    void (*mid)(CellArgs) = cl.guesses ? k_cells_mid<true> : k_cells_mid<false>;
+    static bool mid_ready[2] = {false, false};
+    if (!mid_ready[cl.guesses ? 1 : 0])
+    {
+        cudaFuncSetAttribute(mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mid_smem);
+        mid_ready[cl.guesses ? 1 : 0] = true;
+    }
+    A.big_pass = 1;
+    ++g_launches;
+    mid<<<(unsigned)(148 * 2), kWarpsPerBlock * 32, mid_smem, st>>>(A);
+    A.big_pass = 2;
     ++g_launches;
     if (cl.guesses)
         k_cells_big<true><<<(unsigned)(big_warps() / kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(A);

@@ -23,7 +23,9 @@ enum Status : int
 constexpr int kMaxVertsRef = 64;    // reference MAX_VERTS: more vertices => status vertex_overflow
 constexpr int kCapFast = 64;        // vertex / plane slots of a cell in shared memory
 constexpr int kStackFast = 256;     // pending BVH nodes of a cell in shared memory
-constexpr int kCapBig = 256;        // vertex / plane slots of a deferred cell (global memory)
+constexpr int kCapMid = 128;        // vertex / plane slots of a deferred cell (shared memory, second launch)
+constexpr int kStackMid = 512;
+constexpr int kCapBig = 256;        // vertex / plane slots of a cell that outgrew kCapMid (global memory)
 constexpr int kStackBig = 1024;     // traversal stack of a deferred cell
 constexpr int kCapHuge = 512;       // vertex / plane slots of a cell that outgrew kCapBig (rare)
 constexpr int kStackHuge = 2048;
@@ -137,7 +139,9 @@ struct Workspace
     // cells
     int *rows;            // [N * kRowWidth] directed rows by original index
     int *deg;             // [N] directed degree by original index (kBigFlag: deferred row)
-    int *big_list;        // [N] sorted slots deferred to the large-capacity pass
+    int *big_list;        // [N] sorted slots deferred to the large-capacity passes
+    int *big_list2;       // [big_cap] sorted slots that outgrew the middle tier too
+    int *big_slot2;       // [big_cap] their deferred-row slots
     int *big_rows;        // [big_cap * kBigRowWidth]
     void *big_slabs;      // per-warp state of the large-capacity pass
     void *huge_slabs;     // [kHugeSlabs] state of cells that outgrew the large capacity

@@ -67,6 +67,13 @@ def test_cells_beyond_256_vertices(dev, oracle):
         assert all(np.array_equal(a, b) for a, b in zip(got, exp)), k
         assert (got[2] == 1).sum() == 0
         assert (oracle.cells(c).nverts.max() > 256) == final_over
+        if final_over:
+            # the 512-slot tier integrates its cells too: the volumes partition the box
+            _, _, vol = pg.cell_geometry(torch.from_numpy(c).to(dev))
+            lo, hi = oracle.box(c)
+            box = float(np.prod(hi.astype(np.float64) - lo.astype(np.float64)))
+            v = vol.cpu().numpy().astype(np.float64)
+            assert np.isfinite(v).all() and abs(v.sum() - box) <= 1e-5 * box
 
 
 def test_batch_with_learned_radius_on_lattice_blocks(dev, oracle):

@@ -309,3 +309,19 @@ def test_chunk_environment(dev, monkeypatch, env):
     chunks = pc.last_profile()["chunks"]
     if env.get("PARAGRAM_NUM_CHUNKS") == "4":
         assert chunks == 4
+
+
+def test_search_radius_saves_candidates(dev, oracle):
+    """What a search radius buys: with radii near the exact ones the first pass skips the far
+    candidates of the first leaves (transient clips), the diagram unchanged."""
+    import paragram_b200.cuda as pc
+    from paragram_b200 import workloads as W
+
+    pts = W.clustered(200_000, seed=31)
+    t = torch.from_numpy(pts).to(dev)
+    (a, o, s), st = pc.build_with_stats(t, diagnostics=True)
+    (a2, o2, s2), st2 = pc.build_with_stats(t, radius_hint=st["radius"] * 1.001)
+    assert torch.equal(a, a2) and torch.equal(o, o2) and torch.equal(s, s2)
+    assert st2["hint_misses"] == 0
+    assert st2["candidates"] < 0.8 * st["candidates"], (st2["candidates"], st["candidates"])
+    assert st2["clips"] < st["clips"]
