@@ -32,10 +32,10 @@
 // tested lane-parallel over the vertices.
 //
 // A cell that needs more than 64 vertex / plane slots is deferred to a second
-// launch with 128 slots in shared memory, then to a third with 256 slots in
-// global memory (then 512 if needed); its status is then vertex_overflow (2)
-// if the final cell has more than 64 vertices (the reference MAX_VERTS) and
-// plane_overflow (1) only if even 512 slots overflow.
+// launch with 128 slots in shared memory, and one that outgrows those to a
+// third with 256 slots in global memory (then 512); its status is then
+// vertex_overflow (2) if the final cell has more than 64 vertices (the
+// reference MAX_VERTS) and plane_overflow (1) only if even 512 slots overflow.
 //
 // With a geometry output, each final cell is also integrated before it is
 // discarded (integrate_cell: volume and centroid from a fan of signed
@@ -119,7 +119,7 @@ struct CellArgs
     int *deg;
     int *status;
     int *big_list;
-    int *big_list2;  // cells that outgrew the middle tier too, and their deferred-row slots
+    int *big_list2; // cells that outgrew the middle tier too, and their deferred-row slots
     int *big_slot2;
     int *big_rows;
     int *counters;
@@ -1623,12 +1623,8 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
     if (lane < kNumStats)
         m.cnt[lane] = 0;
     clear_edges(m, lane);
-    // pass 0: the cell range of this launch; pass 1 (middle tier): the cells deferred by
-    // pass 0; pass 2 (large tier): the cells deferred by pass 1, with their row slots
-    const int pass = A.big_pass;
-    int64_t count = pass == 0 ? (A.end - A.begin)
-                              : min((int64_t)A.counters[pass == 1 ? 1 : 5], A.big_cap);
-    int *ctr = &A.counters[pass == 0 ? 0 : (pass == 1 ? 3 : 6)];
+    int64_t count = A.big_pass ? min((int64_t)A.counters[1], A.big_cap) : (A.end - A.begin);
+    int *ctr = A.big_pass ? &A.counters[3] : &A.counters[0];
     for (;;)
     {
         int t = 0;
@@ -1637,24 +1633,24 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
         t = __shfl_sync(kFull, t, 0);
         if (t >= count)
             break;
-        int i = pass == 0 ? (int)(A.begin + t) : (pass == 1 ? A.big_list[t] : A.big_list2[t]);
+        int i = A.big_pass ? A.big_list[t] : (int)(A.begin + t);
         PG_T0(tcell);
         process_cell<CAP, STACK, GUESS, HINT>(m, ws, i, A, lane);
         write_diagnostics(m, ws, A, lane);
-        if (pass)
-            ws.si = pass == 1 ? t : A.big_slot2[t]; // the deferred-row slot
+        if (A.big_pass)
+            ws.si = t; // the deferred-row slot
         if (__any_sync(kFull, ws.flags & kFlagError)) // a flag may be set on any lane
         {
             if (lane == 0)
                 atomicExch(&A.counters[2], 1);
             ws.flags &= ~kFlagError;
         }
-        if (pass == 2 && (ws.flags & kFlagDefer) && ws.si < A.big_cap && huge_cell(A, i, lane, ws.si))
+        if (A.big_pass && (ws.flags & kFlagDefer) && ws.si < A.big_cap && huge_cell(A, i, lane, ws.si))
             continue; // outgrew the 256 slots too: rebuilt with 512
-        if (!(ws.flags & kFlagDefer) || pass == 2)
+        if (!(ws.flags & kFlagDefer) || A.big_pass)
         {
             PG_T0(to);
-            bool done = write_outputs(m, ws, A, lane, pass != 0);
+            bool done = write_outputs(m, ws, A, lane, A.big_pass != 0);
             PG_T1(m, lane, kStatCycOut, to);
             if (done)
             {
@@ -1663,22 +1659,13 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
             }
         }
         PG_COUNT(m, lane, kStatDeferred, 1);
-        // deferred: placeholder outputs (an empty row) until a larger tier rebuilds the cell
+        // deferred: placeholder outputs (an empty row) until the large-capacity pass
         if (lane == 0)
         {
             A.deg[ws.soid] = 0;
             A.status[ws.soid] = kPlaneOverflow;
-            if (pass == 0)
-            {
-                int d = atomicAdd(&A.counters[1], 1);
-                A.big_list[d] = i;
-            }
-            else
-            {
-                int d = atomicAdd(&A.counters[5], 1);
-                A.big_list2[d] = i;
-                A.big_slot2[d] = ws.si;
-            }
+            int d = atomicAdd(&A.counters[1], 1);
+            A.big_list[d] = i;
         }
     }
     flush_stats(m, A, lane);
@@ -1692,6 +1679,89 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) k_cells_fast(CellAr
     cells_body<kCapFast, kStackFast, GUESS, HINT>(mem[w], A, lane);
 }
 
+
+// Rebuild cell i with 256 vertex / plane slots and a 1024-entry queue in this
+// warp's global slab: a cell that outgrew the 128 slots of the middle tier. A
+// cell that outgrows the 256 slots too is rebuilt once more by huge_cell.
+template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, int i, int lane, int slot)
+{
+    size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    auto &m = *reinterpret_cast<CellMem<kCapBig, kStackBig> *>(A.slabs + gw * sizeof(CellMem<kCapBig, kStackBig>));
+    WarpState<kCapBig> ws;
+    if (lane < kNumStats)
+        m.cnt[lane] = 0;
+    clear_edges(m, lane);
+    process_cell<kCapBig, kStackBig, GUESS, false>(m, ws, i, A, lane);
+    write_diagnostics(m, ws, A, lane);
+    if (__any_sync(kFull, ws.flags & kFlagError) && lane == 0)
+        atomicExch(&A.counters[2], 1);
+    if (!((ws.flags & kFlagDefer) && huge_cell(A, i, lane, slot)))
+    {
+        ws.si = slot;
+        write_outputs(m, ws, A, lane, true); // plane_overflow when even the 512 slots ran out
+    }
+    flush_stats(m, A, lane);
+}
+
+// The middle tier's loop: the cells the first pass deferred (list index t =
+// their deferred-row slot), with 128 slots; a cell that outgrows them is listed
+// again for the global-memory tier. A separate body from the first pass's, whose
+// code (one inlined copy of traversal and clip) is kept as it is.
+template <bool GUESS> __device__ __forceinline__ void mid_body(CellMem<kCapMid, kStackMid> &m, const CellArgs &A, int lane)
+{
+    WarpState<kCapMid> ws;
+    if (lane < kNumStats)
+        m.cnt[lane] = 0;
+    clear_edges(m, lane);
+    const int64_t count = min((int64_t)A.counters[1], A.big_cap);
+    for (;;)
+    {
+        int t = 0;
+        if (lane == 0)
+            t = atomicAdd(&A.counters[3], 1);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= count)
+            break;
+        int i = A.big_list[t];
+        process_cell<kCapMid, kStackMid, GUESS, false>(m, ws, i, A, lane);
+        write_diagnostics(m, ws, A, lane);
+        if (__any_sync(kFull, ws.flags & kFlagError) && lane == 0)
+            atomicExch(&A.counters[2], 1);
+        ws.flags &= ~kFlagError;
+        if (ws.flags & kFlagDefer)
+        {
+            // outgrew the 128 slots too: listed, with its row slot, for the launch after this one
+            if (lane == 0)
+            {
+                int d = atomicAdd(&A.counters[5], 1);
+                A.big_list2[d] = i;
+                A.big_slot2[d] = t;
+            }
+            continue;
+        }
+        ws.si = t;
+        write_outputs(m, ws, A, lane, true);
+    }
+    flush_stats(m, A, lane);
+}
+
+// Global-memory tier: the cells that outgrew the middle tier, one per warp at a time.
+template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_cells_big(CellArgs A)
+{
+    int lane = threadIdx.x & 31;
+    const int64_t count = min((int64_t)A.counters[5], A.big_cap);
+    for (;;)
+    {
+        int t = 0;
+        if (lane == 0)
+            t = atomicAdd(&A.counters[6], 1);
+        t = __shfl_sync(kFull, t, 0);
+        if (t >= count)
+            break;
+        big_cell<GUESS>(A, A.big_list2[t], lane, A.big_slot2[t]);
+    }
+}
+
 // Middle tier: the cells that outgrew 64 slots, with 128 slots and a 512-entry
 // queue in shared memory (its own launch, so its larger shared-memory carve-out
 // does not shrink the first pass's L1).
@@ -1700,15 +1770,7 @@ template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) 
     extern __shared__ __align__(16) unsigned char mid_smem[];
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     auto *m = reinterpret_cast<CellMem<kCapMid, kStackMid> *>(mid_smem) + w;
-    cells_body<kCapMid, kStackMid, GUESS, false>(*m, A, lane);
-}
-
-template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_cells_big(CellArgs A)
-{
-    int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    size_t gw = (size_t)blockIdx.x * kWarpsPerBlock + w;
-    auto *m = reinterpret_cast<CellMem<kCapBig, kStackBig> *>(A.slabs + gw * sizeof(CellMem<kCapBig, kStackBig>));
-    cells_body<kCapBig, kStackBig, GUESS, false>(*m, A, lane);
+    mid_body<GUESS>(*m, A, lane);
 }
 
 int big_warps() { return 148 * kMaxWarpsPerSM; } // one slab per resident warp
@@ -1789,9 +1851,9 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
     kern<<<(unsigned)grid, kWarpsPerBlock * 32, 0, st>>>(A);
 }
 
-// The deferred counts stay on the device: fixed grids read them. Pass 1 (middle
-// tier, shared memory) rebuilds the cells pass 0 deferred; pass 2 (global slabs)
-// the ones that outgrew it too.
+// The deferred counts stay on the device: fixed grids read them. The middle
+// tier (shared memory) rebuilds the cells the first pass deferred; the global
+// tier (256, then 512 slots) the ones that outgrow it.
 void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, int64_t big_cap, cudaStream_t st)
 {
     CellArgs A = make_args(ws, cl);
@@ -1805,15 +1867,15 @@ void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, in
         cudaFuncSetAttribute(mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mid_smem);
         mid_ready[cl.guesses ? 1 : 0] = true;
     }
-    A.big_pass = 1;
     ++g_launches;
     mid<<<(unsigned)(148 * 2), kWarpsPerBlock * 32, mid_smem, st>>>(A);
-    A.big_pass = 2;
+    // one global slab per warp of this grid
+    unsigned grid = (unsigned)(big_warps() / kWarpsPerBlock);
     ++g_launches;
     if (cl.guesses)
-        k_cells_big<true><<<(unsigned)(big_warps() / kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(A);
+        k_cells_big<true><<<grid, kWarpsPerBlock * 32, 0, st>>>(A);
     else
-        k_cells_big<false><<<(unsigned)(big_warps() / kWarpsPerBlock), kWarpsPerBlock * 32, 0, st>>>(A);
+        k_cells_big<false><<<grid, kWarpsPerBlock * 32, 0, st>>>(A);
 }
 
 } // namespace pg

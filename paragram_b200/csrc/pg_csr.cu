@@ -25,6 +25,26 @@ __device__ __forceinline__ const int *row_of(const int *rows, const int *big_row
     return rows + (size_t)u * kRowWidth;
 }
 
+// Whether the sorted row r[0, d) lists x, for d <= kRowWidth: one pass of independent
+// 16-byte loads over the row (a single round trip to L2, where a binary search would make
+// four dependent ones). Rows start 16-byte aligned (kRowWidth = 36 ints, deferred rows
+// kBigRowWidth) and the loads stay within the row's first kRowWidth slots.
+__device__ __forceinline__ bool row_has_scan(const int *r, int d, int x)
+{
+    const int4 *r4 = reinterpret_cast<const int4 *>(r);
+    bool hit = false;
+#pragma unroll
+    for (int k = 0; k < kRowWidth / 4; ++k)
+    {
+        if (4 * k >= d)
+            break;
+        int4 q = __ldg(r4 + k);
+        hit = hit || (q.x == x && 4 * k < d) || (q.y == x && 4 * k + 1 < d) || (q.z == x && 4 * k + 2 < d) ||
+              (q.w == x && 4 * k + 3 < d);
+    }
+    return hit;
+}
+
 __device__ __forceinline__ bool row_has(const int *r, int d, int x)
 {
     int lo = 0, hi = d;
@@ -67,7 +87,7 @@ __global__ void k_csr_count(const int *__restrict__ rows, const int *__restrict_
         if (dv <= 0)
             continue;
         ++kept;
-        bool missing = !row_has(rv, dv, u);
+        bool missing = !(dv <= kRowWidth ? row_has_scan(rv, dv, u) : row_has(rv, dv, u));
         if (missing)
             atomicAdd(&miss[v], 1);
         if (k < 64)
@@ -89,15 +109,17 @@ __global__ void k_csr_sizes(const int *__restrict__ cnt, const int *__restrict__
         sizes[u] = (uint32_t)(cnt[u] + miss[u]);
 }
 
+// The fill reads no neighbour row (the count's masks decided every entry): rows are taken in
+// their own order, so that reads of the rows and writes of the adjacency are contiguous.
 __global__ void k_csr_fill(const int *__restrict__ rows, const int *__restrict__ big_rows, const int *__restrict__ deg,
-                           const int *__restrict__ oid, int64_t n, const int *__restrict__ off,
-                           const int *__restrict__ cnt, const unsigned long long *__restrict__ masks,
-                           int *__restrict__ fill, int *__restrict__ adj)
+                           int64_t n, const int *__restrict__ off, const int *__restrict__ cnt,
+                           const unsigned long long *__restrict__ masks, int *__restrict__ fill,
+                           int *__restrict__ adj)
 {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n)
         return;
-    int u = oid[t], d;
+    int u = (int)t, d;
     const int *r = row_of(rows, big_rows, deg, u, d);
     int pos = off[u];
     if (d <= 64)
@@ -161,8 +183,7 @@ void csr_fill(const Workspace &ws, int64_t n, const int32_t *offsets, int32_t *a
     unsigned g = (unsigned)((n + 255) / 256);
     cudaMemsetAsync(ws.fill, 0, sizeof(int) * (size_t)n, st);
     ++g_launches;
-    k_csr_fill<<<g, 256, 0, st>>>(ws.rows, ws.big_rows, ws.deg, ws.oid, n, offsets, ws.cnt, ws.rmask, ws.fill,
-                                  adjacency);
+    k_csr_fill<<<g, 256, 0, st>>>(ws.rows, ws.big_rows, ws.deg, n, offsets, ws.cnt, ws.rmask, ws.fill, adjacency);
     ++g_launches;
     k_csr_sort<<<g, 256, 0, st>>>(ws.miss, n, offsets, adjacency);
 }

@@ -1,7 +1,8 @@
 """Facet areas (pg_face_areas, from the exported vertices), checked by identities.
 
 * The facet between u and v is one polygon: the area of entry u->v equals that
-  of v->u (relative 1e-4).
+  of v->u (relative 1e-4, plus 1e-7 of the mean facet area for thin facets:
+  each side rounds the vertices relative to its own point).
 * Divergence theorem for every cell that no box face bounds: its volume (from
   the cell kernel's own integration, an independent computation) equals
   (1/3) sum_f A_f h_f over its facets, h_f the signed distance from the cell's
@@ -55,8 +56,11 @@ def test_face_areas_identities(dev, case):
     found = key[order][pos] == rkey
     assert found.all()
     b = a[order][pos]
-    scale = np.maximum(np.maximum(a, b), 1e-30)
-    assert (np.abs(a - b) <= 1e-4 * scale + 1e-12).all(), np.abs(a - b).max()
+    scale = np.maximum(a, b)
+    # FP32 rounding of the vertices relative to each cell's point: relative 1e-4 on ordinary facets,
+    # plus an absolute floor of 1e-7 of the mean facet area for the thinnest ones
+    floor = 1e-7 * a.mean()
+    assert (np.abs(a - b) <= 1e-4 * scale + floor).all(), np.abs(a - b).max()
     # divergence theorem on cells bounded by bisectors only
     p = pts.astype(np.float64)
     ww = np.zeros(n) if w is None else w.astype(np.float64)
