@@ -123,7 +123,10 @@ typedef struct pg_model
     float target_mean[2];
     float target_scale[2];
     float radius_margin;   /* added to the predicted log radius */
-    float pad[3];
+    float route_degree;    /* > 0: a point whose predicted neighbour count is at least this skips the
+                              first pass (64 vertex slots) and is built by the 128-slot tier directly;
+                              0: off. The diagram does not depend on it. */
+    float pad[2];
     float b1[64];
     float b2[64];
     float b3[8];           /* entries 2..7 unused */
@@ -175,9 +178,26 @@ int pg_emit_adjacency(int64_t num_points, const void *workspace, const int32_t *
  * (the reference only prints timings, voronoi_ultra.cu:196-219). */
 int pg_stats(const void *workspace, int64_t num_points, uint64_t *out, int32_t count, void *stream);
 
+/* Where the BVH lives inside a workspace that pg_build (num_clouds = 1) or pg_build_batch
+ * filled: out[k] = byte offset from the workspace's start of
+ *   [0] the sorted points (float4 x, y, z, w per sorted slot, N of them),
+ *   [1] sorted slot -> original point index (int32 [N]),
+ *   [2] the traversal records, 4 float4 per internal node (node i at 64 i bytes):
+ *       (c0.lo.x, c0.lo.y, c0.lo.z, c0.hi.x), (c0.hi.y, c0.hi.z, c1.lo.x, c1.lo.y),
+ *       (c1.lo.z, c1.hi.x, c1.hi.y, c1.hi.z), (ref0, ref1 as int32 bits, maxw0, maxw1);
+ *       a reference < 0 is a leaf: bit 31, count - 1 in bits 26..30, first sorted slot in
+ *       bits 0..25; a reference >= 0 is another record,
+ *   [3] the root reference of each cloud (int32 [num_clouds]),
+ *   [4] each cloud's box (float32 [8 per cloud]: lo xyz, hi xyz, max weight, unused).
+ * For inspection and tests (the layout depends on num_points and num_clouds only).
+ * No reference counterpart (the reference's BVH is cuBQL's, pwr_bvh.cu:42-339). */
+int pg_workspace_tree(int64_t num_points, int32_t num_clouds, int64_t *out, int32_t count);
+
 /* Profile of the last pg_build + pg_emit_adjacency on this thread:
  * out[0] kernel launches, out[1] LBVH ms, out[2] cell pass ms, out[3] deferred-cell
- * pass ms, out[4] CSR count + scan ms, out[5] deferred cells, out[6] cell-pass chunks.
+ * pass ms, out[4] CSR count + scan ms, out[5] deferred cells, out[6] cell-pass chunks,
+ * out[7] deferred cells rebuilt with 256 slots, out[8] with 512 slots, out[9] cells a
+ * learned model routed past the first pass (pg_model.route_degree).
  * The times are recorded only when options->debug != 0 (CUDA events on the stream).
  * No reference counterpart (the reference prints timings with debug=True,
  * voronoi_ultra.cu:196-219, 368-373). */

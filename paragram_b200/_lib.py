@@ -7,7 +7,9 @@ import os
 import threading
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libparagram_b200.so")
+#: The library loaded by ``load()``; ``PARAGRAM_B200_LIB`` names another build of the same sources
+#: (the phase-cycle instrumented one, ``python -m paragram_b200.build --phase-cycles``).
+LIB_PATH = os.environ.get("PARAGRAM_B200_LIB") or os.path.join(_HERE, "libparagram_b200.so")
 
 _lock = threading.Lock()
 _lib = None
@@ -41,7 +43,7 @@ class PgOptions(ctypes.Structure):
 EXPORTED = ["pg_version", "pg_last_error", "pg_workspace_size", "pg_build", "pg_emit_adjacency", "pg_stats",
             "pg_last_profile", "pg_degrees_to_offsets_noalloc", "pg_batch_workspace_size", "pg_build_batch",
             "pg_batch_check", "pg_mlp_num_params", "pg_mlp_model_bytes", "pg_mlp_forward", "pg_mlp_grad",
-            "pg_mlp_adam", "pg_mlp_pack", "pg_face_areas"]
+            "pg_mlp_adam", "pg_mlp_pack", "pg_face_areas", "pg_workspace_tree"]
 
 
 def load() -> ctypes.CDLL:
@@ -68,6 +70,8 @@ def load() -> ctypes.CDLL:
         lib.pg_emit_adjacency.restype = ctypes.c_int
         lib.pg_stats.argtypes = [vp, i64, ctypes.POINTER(ctypes.c_uint64), i32, vp]
         lib.pg_stats.restype = ctypes.c_int
+        lib.pg_workspace_tree.argtypes = [i64, i32, ctypes.POINTER(i64), i32]
+        lib.pg_workspace_tree.restype = ctypes.c_int
         lib.pg_last_profile.argtypes = [ctypes.POINTER(ctypes.c_double), i32]
         lib.pg_last_profile.restype = ctypes.c_int
         lib.pg_batch_workspace_size.argtypes = [i64, i32, ctypes.POINTER(sz)]

@@ -19,6 +19,10 @@ BUILD_DIR = os.path.join(HERE, "_build")
 LIB_PATH = os.path.join(HERE, "libparagram_b200.so")
 SOURCES = ["pg_api.cu", "pg_lbvh.cu", "pg_cells.cu", "pg_csr.cu", "pg_scan.cu", "pg_noalloc.cu", "pg_mlp.cu",
            "pg_faces.cu"]
+#: The instrumented variant (per-phase SM cycle counters in the cell kernel, -DPG_PHASE_CYCLES): a
+#: separate library for profiling only; ``PARAGRAM_B200_LIB`` selects it at load time.
+PHASE_BUILD_DIR = os.path.join(HERE, "_build_phase")
+PHASE_LIB_PATH = os.path.join(HERE, "libparagram_b200_phase.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
@@ -36,16 +40,18 @@ def _deps() -> list[str]:
     ]
 
 
-def up_to_date() -> bool:
-    if not os.path.exists(LIB_PATH):
+def up_to_date(lib: str = LIB_PATH) -> bool:
+    if not os.path.exists(lib):
         return False
-    t = os.path.getmtime(LIB_PATH)
+    t = os.path.getmtime(lib)
     return all(os.path.getmtime(d) <= t for d in _deps() if os.path.exists(d))
 
 
-def _compile(src: str, ptxas_verbose: bool) -> tuple[str, str]:
-    obj = os.path.join(BUILD_DIR, os.path.splitext(src)[0] + ".o")
+def _compile(src: str, ptxas_verbose: bool, phase_cycles: bool = False) -> tuple[str, str]:
+    obj = os.path.join(PHASE_BUILD_DIR if phase_cycles else BUILD_DIR, os.path.splitext(src)[0] + ".o")
     cmd = [nvcc(), *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+    if phase_cycles:
+        cmd.append("-DPG_PHASE_CYCLES")
     if ptxas_verbose:
         cmd += ["-Xptxas", "-v"]
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -54,27 +60,29 @@ def _compile(src: str, ptxas_verbose: bool) -> tuple[str, str]:
     return obj, r.stderr
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
-    """Compile the CUDA library for sm_100a if it is missing or stale."""
-    if not force and up_to_date():
-        return LIB_PATH
-    os.makedirs(BUILD_DIR, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False, phase_cycles: bool = False) -> str:
+    """Compile the CUDA library for sm_100a if it is missing or stale (``phase_cycles``: the
+    instrumented variant, ``libparagram_b200_phase.so``)."""
+    lib_path = PHASE_LIB_PATH if phase_cycles else LIB_PATH
+    if not force and up_to_date(lib_path):
+        return lib_path
+    os.makedirs(PHASE_BUILD_DIR if phase_cycles else BUILD_DIR, exist_ok=True)
     with concurrent.futures.ThreadPoolExecutor(max_workers=len(SOURCES)) as ex:
-        results = list(ex.map(lambda s: _compile(s, ptxas_verbose), SOURCES))
+        results = list(ex.map(lambda s: _compile(s, ptxas_verbose, phase_cycles), SOURCES))
     if verbose or ptxas_verbose:
         for _, log in results:
             if log:
                 print(log, file=sys.stderr)
     objs = [o for o, _ in results]
-    tmp = LIB_PATH + ".tmp"
+    tmp = lib_path + ".tmp"
     cmd = [nvcc(), *ARCH, "-shared", "-o", tmp, *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"nvcc link failed:\n{r.stderr}")
-    os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+    os.replace(tmp, lib_path)
+    return lib_path
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True, ptxas_verbose="--ptxas" in sys.argv)
-    print(LIB_PATH)
+    print(build(force="--force" in sys.argv, verbose=True, ptxas_verbose="--ptxas" in sys.argv,
+                phase_cycles="--phase-cycles" in sys.argv))

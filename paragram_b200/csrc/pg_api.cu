@@ -21,7 +21,7 @@ namespace pg
 
 static thread_local std::string g_last_error;
 thread_local long long g_launches = 0;
-static thread_local double g_profile[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+static thread_local double g_profile[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 
 static int fail(int code, const std::string &msg)
 {
@@ -37,7 +37,12 @@ int set_last_error(int code, const std::string &msg)
 
 static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static int64_t big_cap(int64_t n) { return std::min<int64_t>(n, 65536 + n / 32); }
+// Deferred-row slots: room for the cells that outgrow the first pass's 64 slots
+// (65536 + n / 32) plus the cells a learned model routes to the 128-slot tier
+// directly (at most route_cap, so that routing never exhausts the room of the
+// cells that overflow).
+static int64_t route_cap(int64_t n) { return std::min<int64_t>(n, 4096 + n / 128); }
+static int64_t big_cap(int64_t n) { return std::min<int64_t>(n, 65536 + n / 32 + route_cap(n)); }
 
 size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
 {
@@ -150,12 +155,13 @@ __global__ void k_single_cloud(int *off, int n)
     off[1] = n;
 }
 
-// search radius per sorted slot from the caller's per-point radii
+// search radius per sorted slot from the caller's per-point radii (negative and NaN radii:
+// none; a negative hint is the model's routing mark)
 __global__ void k_hint_gather(int64_t n, const int *oid, const float *radius, float *hint)
 {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
-        hint[i] = radius[oid[i]];
+        hint[i] = fmaxf(radius[oid[i]], 0.0f);
 }
 
 static int check_counters(const int *host, int64_t n)
@@ -264,6 +270,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     cl.weighted = weights != nullptr;
     cl.min_blocks = opt.blocks_per_sm == 3 ? 3 : 2; // register budget of the cell kernel
     cl.big_cap = big_cap(n);
+    cl.route_cap = route_cap(n);
     cl.fp32_only = opt.predicates == 1;
     cl.radius_out = opt.radius_out;
     cl.work_out = opt.work_out;
@@ -314,12 +321,12 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         cudaError_t e = cudaGetLastError();
         return e == cudaSuccess ? PG_OK : fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
     }
-    int host[4] = {0, 0, 0, 0};
+    int host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int64_t edges = 0;
     {
         uint32_t e32 = 0;
         cudaMemcpyAsync(&e32, offsets + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(host, ws.counters, 4 * sizeof(int), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(host, ws.counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, st);
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess)
             return fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
@@ -349,6 +356,9 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
             cudaEventDestroy(e);
     }
     g_profile[5] = (double)host[1];
+    g_profile[7] = (double)host[5];                                 // rebuilt with 256 slots
+    g_profile[8] = (double)std::min(host[4], kHugeSlabs);           // rebuilt with 512 slots
+    g_profile[9] = (double)std::min<int64_t>(host[7], route_cap(n)); // routed past the first pass
     int rc = check_counters(host, n);
     if (rc != PG_OK)
         return rc;
@@ -385,6 +395,21 @@ int pg_build(int64_t n, const float *points, const float *weights, const int32_t
         return pg::fail(PG_ERR_INVALID, "num_edges must not be NULL");
     return pg::build_impl(n, 1, nullptr, points, weights, guesses, guess_off, options, workspace, workspace_bytes,
                           offsets, status, num_edges, stream);
+}
+
+int pg_workspace_tree(int64_t num_points, int32_t num_clouds, int64_t *out, int32_t count)
+{
+    if (!out || count < 0 || num_clouds < 1 || num_points < 0 || num_points >= pg::kMaxPoints)
+        return pg::fail(PG_ERR_INVALID, "need out != NULL, count >= 0, num_clouds >= 1 and num_points in [0, 2^26)");
+    // the layout from a stand-in base address; only differences from it are used
+    char *base = reinterpret_cast<char *>((uintptr_t)1 << 40);
+    pg::Workspace w;
+    pg::workspace_layout(num_points, num_clouds, base, &w);
+    const char *ptrs[5] = {(const char *)w.pts, (const char *)w.oid, (const char *)w.records,
+                           (const char *)w.cloud_root, (const char *)w.box};
+    for (int k = 0; k < count && k < 5; ++k)
+        out[k] = (int64_t)(ptrs[k] - base);
+    return pg::set_last_error(PG_OK, "");
 }
 
 int pg_batch_workspace_size(int64_t total_points, int32_t num_clouds, size_t *bytes)
@@ -446,7 +471,7 @@ int pg_last_profile(double *out, int32_t count)
 {
     if (!out || count < 0)
         return pg::fail(PG_ERR_INVALID, "bad arguments");
-    for (int i = 0; i < count && i < 8; ++i)
+    for (int i = 0; i < count && i < 10; ++i)
         out[i] = pg::g_profile[i];
     return PG_OK;
 }

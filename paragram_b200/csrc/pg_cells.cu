@@ -40,6 +40,7 @@
 // With a geometry output, each final cell is also integrated before it is
 // discarded (integrate_cell: volume and centroid from a fan of signed
 // tetrahedra per face).
+#include <atomic>
 #include <cfloat>
 #include <climits>
 #include <type_traits>
@@ -127,6 +128,7 @@ struct CellArgs
     int64_t begin, end;
     int big_pass;
     int64_t big_cap;
+    int64_t route_cap;
     char *slabs;
     char *huge_slabs;
     float *radius_out; // optional per-cell diagnostics (original ids)
@@ -1272,6 +1274,21 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
     if (A.hint != nullptr)
     {
         float rq = A.hint[i];
+        if (rq < 0.0f)
+        {
+            // the model predicts more neighbours than the first pass's slots hold: deferred
+            // to the 128-slot tier before any traversal, while the routing share of the
+            // deferred rows lasts
+            int r = 0;
+            if (lane == 0)
+                r = atomicAdd(&A.counters[7], 1);
+            if (__shfl_sync(kFull, r, 0) < A.route_cap)
+            {
+                ws.flags |= kFlagDefer;
+                return;
+            }
+            rq = -rq;
+        }
         if (rq > 0.0f && rq < 1e30f)
             cap = rq;
     }
@@ -1587,6 +1604,17 @@ template <int CAP, int STACK> __device__ void flush_stats(CellMem<CAP, STACK> &m
         atomicAdd(&A.stats[lane], m.cnt[lane]);
 }
 
+// The per-phase cycle counters describe the first pass; a deferred tier reports
+// only its total (kStatCycBig).
+template <int CAP, int STACK> __device__ __forceinline__ void deferred_phase_counters(CellMem<CAP, STACK> &m, int lane)
+{
+#ifdef PG_PHASE_CYCLES
+    if (lane >= kStatCycCell && lane <= kStatCycOut)
+        m.cnt[lane] = 0;
+    __syncwarp();
+#endif
+}
+
 // Rebuild cell i with 512 vertex / plane slots and a 2048-entry queue: the
 // rare cell that outgrew the 256 slots (long cells of surface data reach a
 // few hundred vertices). Its state lives in one of kHugeSlabs global slabs,
@@ -1612,6 +1640,7 @@ __device__ __noinline__ bool huge_cell(const CellArgs &A, int i, int lane, int s
         atomicExch(&A.counters[2], 1);
     ws.si = slot;
     write_outputs(m, ws, A, lane, true);
+    deferred_phase_counters(m, lane);
     flush_stats(m, A, lane);
     return true;
 }
@@ -1658,6 +1687,7 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
                 continue;
             }
         }
+        PG_T1(m, lane, kStatCycCell, tcell);
         PG_COUNT(m, lane, kStatDeferred, 1);
         // deferred: placeholder outputs (an empty row) until the large-capacity pass
         if (lane == 0)
@@ -1690,6 +1720,7 @@ template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, i
     WarpState<kCapBig> ws;
     if (lane < kNumStats)
         m.cnt[lane] = 0;
+    PG_T0(tb);
     clear_edges(m, lane);
     process_cell<kCapBig, kStackBig, GUESS, false>(m, ws, i, A, lane);
     write_diagnostics(m, ws, A, lane);
@@ -1700,6 +1731,8 @@ template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, i
         ws.si = slot;
         write_outputs(m, ws, A, lane, true); // plane_overflow when even the 512 slots ran out
     }
+    PG_T1(m, lane, kStatCycBig, tb);
+    deferred_phase_counters(m, lane);
     flush_stats(m, A, lane);
 }
 
@@ -1723,6 +1756,7 @@ template <bool GUESS> __device__ __forceinline__ void mid_body(CellMem<kCapMid, 
         if (t >= count)
             break;
         int i = A.big_list[t];
+        PG_T0(tb);
         process_cell<kCapMid, kStackMid, GUESS, false>(m, ws, i, A, lane);
         write_diagnostics(m, ws, A, lane);
         if (__any_sync(kFull, ws.flags & kFlagError) && lane == 0)
@@ -1737,11 +1771,14 @@ template <bool GUESS> __device__ __forceinline__ void mid_body(CellMem<kCapMid, 
                 A.big_list2[d] = i;
                 A.big_slot2[d] = t;
             }
+            PG_T1(m, lane, kStatCycBig, tb);
             continue;
         }
         ws.si = t;
         write_outputs(m, ws, A, lane, true);
+        PG_T1(m, lane, kStatCycBig, tb);
     }
+    deferred_phase_counters(m, lane);
     flush_stats(m, A, lane);
 }
 
@@ -1805,6 +1842,7 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.end = cl.cell_end;
     A.big_pass = 0;
     A.big_cap = 0;
+    A.route_cap = 0;
     A.slabs = (char *)ws.big_slabs;
     A.huge_slabs = (char *)ws.huge_slabs;
     A.radius_out = cl.radius_out;
@@ -1841,6 +1879,7 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
     if (blocks_per_sm < 1)
         blocks_per_sm = 1;
     A.big_cap = cl.big_cap;
+    A.route_cap = cl.route_cap;
     int64_t grid = std::min<int64_t>((int64_t)num_sms * blocks_per_sm, big_warps() / kWarpsPerBlock);
     int64_t need = (cells + kWarpsPerBlock - 1) / kWarpsPerBlock;
     if (grid > need)
@@ -1861,11 +1900,15 @@ void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, in
     A.big_cap = big_cap;
     const size_t mid_smem = sizeof(CellMem<kCapMid, kStackMid>) * kWarpsPerBlock;
     void (*mid)(CellArgs) = cl.guesses ? k_cells_mid<true> : k_cells_mid<false>;
-    static bool mid_ready[2] = {false, false};
-    if (!mid_ready[cl.guesses ? 1 : 0])
+    // the shared-memory opt-in is a per-device attribute of the kernel: set once per device
+    static std::atomic<unsigned long long> mid_ready[2];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(mid_ready[cl.guesses ? 1 : 0].load() & bit))
     {
         cudaFuncSetAttribute(mid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mid_smem);
-        mid_ready[cl.guesses ? 1 : 0] = true;
+        mid_ready[cl.guesses ? 1 : 0].fetch_or(bit);
     }
     ++g_launches;
     mid<<<(unsigned)(148 * 2), kWarpsPerBlock * 32, mid_smem, st>>>(A);

@@ -35,6 +35,7 @@ struct CellLaunch
     int weighted;
     int min_blocks; // register-budget variant of the cell kernel (2 or 3 blocks per SM)
     int64_t big_cap; // deferred-row slots
+    int64_t route_cap; // of which at most this many for cells the model routes past the first pass
     float *radius_out; // per original id: certified radius of the final cell, or nullptr
     int *work_out;     // per original id: nodes, leaves, candidates, peak queue; or nullptr
     float *geometry_out; // per original id: centroid x, y, z and volume of the cell; or nullptr

@@ -229,7 +229,7 @@ struct MlpSmem
     __nv_bfloat16 w3t[kH * kS16]; // [in][out], columns 2..15 zero
     float b1[kH], b2[kH], b3[8];
     float mean[kF], scale[kF];
-    float tmean[kO], tscale[kO], margin;
+    float tmean[kO], tscale[kO], margin, route;
 };
 
 __device__ void load_model(MlpSmem &S, const pg_model *M, bool transposed)
@@ -278,6 +278,7 @@ __device__ void load_model(MlpSmem &S, const pg_model *M, bool transposed)
     }
     if (threadIdx.x == 0)
         S.margin = M->radius_margin;
+        S.route = M->route_degree;
 }
 
 // Forward pass of one 16-row tile. ax: A fragments of the normalized BF16
@@ -422,7 +423,11 @@ __global__ void __launch_bounds__(256) k_mlp_predict(int64_t n, const float4 *__
                     {
                         float ly = F.y[2 * h] / S.tscale[0] + S.tmean[0] + S.margin + lref_r;
                         float rad = expf(ly);
-                        hint[ir] = (lref_r == lref_r && rad < 1e30f) ? rad : 0.0f;
+                        // a predicted neighbour count at or above route_degree: negative radius,
+                        // the cell pass sends the cell to its 128-slot tier directly
+                        float deg = (F.y[2 * h + 1] / S.tscale[1] + S.tmean[1]) * 16.0f;
+                        bool route = S.route > 0.0f && deg >= S.route;
+                        hint[ir] = (lref_r == lref_r && rad < 1e30f) ? (route ? -rad : rad) : 0.0f;
                     }
                 }
             }

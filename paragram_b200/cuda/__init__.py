@@ -27,7 +27,8 @@ STAT_NAMES = ["tests", "fp64_escalations", "exact_escalations", "deferred_cells"
 _last_stats: dict = {}
 _last_diag: dict = {}
 #: Names of the values returned by ``last_profile()`` (pg_last_profile in include/paragram_b200.h).
-PROFILE_NAMES = ["launches", "lbvh_ms", "cells_ms", "deferred_ms", "csr_ms", "deferred_cells", "chunks"]
+PROFILE_NAMES = ["launches", "lbvh_ms", "cells_ms", "deferred_ms", "csr_ms", "deferred_cells", "chunks",
+                 "deferred_256", "deferred_512", "routed_cells"]
 
 
 def _check(ok: bool, msg: str):

@@ -39,7 +39,7 @@ NPARAM = 5378
 MODEL_BYTES = 11984
 MAGIC = 0x314D4750
 # byte offsets inside pg_model (include/paragram_b200.h)
-_OFF_FEAT_MEAN, _OFF_FEAT_SCALE, _OFF_TMEAN, _OFF_TSCALE, _OFF_MARGIN = 16, 80, 144, 152, 160
+_OFF_FEAT_MEAN, _OFF_FEAT_SCALE, _OFF_TMEAN, _OFF_TSCALE, _OFF_MARGIN, _OFF_ROUTE = 16, 80, 144, 152, 160, 164
 _LAYOUT = [("w1", (64, 16)), ("b1", (64,)), ("w2", (64, 64)), ("b2", (64,)), ("w3", (2, 64)), ("b3", (2,))]
 
 
@@ -118,7 +118,9 @@ class Model:
     def _stream(self):
         return torch.cuda.current_stream(self.device).cuda_stream
 
-    def _header(self, mean, scale, tmean, tscale, margin):
+    def _header(self, mean, scale, tmean, tscale, margin, route_degree=None):
+        if route_degree is None:
+            route_degree = getattr(self, "route_degree", 0.0)
         head = np.zeros(176, dtype=np.uint8)
         head[0:16] = np.array([MAGIC, 16, 64, 0], dtype=np.uint32).view(np.uint8)
         head[_OFF_FEAT_MEAN:_OFF_FEAT_MEAN + 64] = np.asarray(mean, np.float32).view(np.uint8)
@@ -126,7 +128,9 @@ class Model:
         head[_OFF_TMEAN:_OFF_TMEAN + 8] = np.asarray(tmean, np.float32).view(np.uint8)
         head[_OFF_TSCALE:_OFF_TSCALE + 8] = np.asarray(tscale, np.float32).view(np.uint8)
         head[_OFF_MARGIN:_OFF_MARGIN + 4] = np.asarray([margin], np.float32).view(np.uint8)
+        head[_OFF_ROUTE:_OFF_ROUTE + 4] = np.asarray([route_degree], np.float32).view(np.uint8)
         self.blob[:176].copy_(torch.from_numpy(head))
+        self.route_degree = float(route_degree)
         self.feat_mean, self.feat_scale = np.asarray(mean, np.float32), np.asarray(scale, np.float32)
         self.target_mean, self.target_scale = np.asarray(tmean, np.float32), np.asarray(tscale, np.float32)
         self.margin = float(margin)
@@ -193,6 +197,19 @@ class Model:
         self._header(self.feat_mean, self.feat_scale, self.target_mean, self.target_scale, margin)
         return margin
 
+    def set_route(self, degree: float = 0.0):
+        """Route the cells whose predicted neighbour count is at least ``degree`` past the first pass
+        (its 64 vertex slots) straight to the 128-slot tier; 0 turns routing off. A cell with more
+        than 34 faces has more than 64 vertices, so thresholds in the mid thirties target the cells
+        the first pass would give up on. The diagram never depends on it."""
+        self._header(self.feat_mean, self.feat_scale, self.target_mean, self.target_scale, self.margin,
+                     float(degree))
+
+    def predicted_degree(self, x: torch.Tensor) -> torch.Tensor:
+        """Predicted neighbour count for raw features [N, 16]."""
+        y = self.predict(x)[:, 1].double()
+        return (y / float(self.target_scale[1]) + float(self.target_mean[1])) * 16.0
+
     def hit_rate(self, data: Samples) -> float:
         """Fraction of cells whose certified radius lies within the calibrated prediction."""
         ok = data.weights > 0
@@ -201,14 +218,15 @@ class Model:
 
     def state_dict(self) -> dict:
         return {"params": self.params.cpu().numpy(), "feat_mean": self.feat_mean, "feat_scale": self.feat_scale,
-                "target_mean": self.target_mean, "target_scale": self.target_scale, "margin": self.margin}
+                "target_mean": self.target_mean, "target_scale": self.target_scale, "margin": self.margin,
+                "route_degree": self.route_degree}
 
     @classmethod
     def from_state(cls, state: dict, device) -> "Model":
         m = cls(device)
         m.params.copy_(torch.from_numpy(np.asarray(state["params"], np.float32)))
         m._header(state["feat_mean"], state["feat_scale"], state["target_mean"], state["target_scale"],
-                  float(state["margin"]))
+                  float(state["margin"]), float(state.get("route_degree", 0.0)))
         lib = _lib.load()
         with torch.cuda.device(m.device):
             _check(lib, lib.pg_mlp_pack(m.params.data_ptr(), m.blob.data_ptr(), m._stream()))

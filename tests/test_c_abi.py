@@ -119,3 +119,22 @@ def test_options_layout_matches_header(tmp_path):
     vals = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     assert vals[0] == ctypes.sizeof(_lib.PgOptions)
     assert vals[1:] == [getattr(_lib.PgOptions, f).offset for f in fields]
+
+
+def test_workspace_tree_offsets(lib):
+    out = (ctypes.c_int64 * 5)()
+    for n, clouds in ((1000, 1), (250_000, 1), (250_000, 37)):
+        size = ctypes.c_size_t(0)
+        if clouds == 1:
+            assert lib.pg_workspace_size(n, ctypes.byref(size)) == 0
+        else:
+            assert lib.pg_batch_workspace_size(n, clouds, ctypes.byref(size)) == 0
+        assert lib.pg_workspace_tree(n, clouds, out, 5) == 0
+        offs = list(out)
+        assert all(o % 256 == 0 for o in offs)
+        # points, order and records are N-sized; the per-cloud roots and boxes come last
+        assert offs[0] + 16 * n <= offs[1] and offs[1] + 4 * n <= offs[2] < offs[3]
+        assert offs[3] + 4 * clouds <= size.value and offs[4] + 32 * clouds <= size.value
+    assert lib.pg_workspace_tree(1000, 0, out, 5) == -1
+    assert lib.pg_workspace_tree(-1, 1, out, 5) == -1
+    assert lib.pg_workspace_tree(1000, 1, None, 5) == -1

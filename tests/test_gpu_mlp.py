@@ -146,3 +146,49 @@ def test_training_and_learned_build(dev, oracle):
     dp = learned.power_diagram(torch.from_numpy(wpts).to(dev), tw, model)
     pp = pg.power_diagram(torch.from_numpy(wpts).to(dev), tw)
     assert torch.equal(dp.adjacency, pp.adjacency) and torch.equal(dp.status, pp.status)
+
+
+def test_learned_routing(dev, oracle):
+    """The model's neighbour-count output routes work: with route_degree set, the cells predicted at
+    or above it skip the first pass (64 vertex slots) and are built by the 128-slot tier. The diagram
+    is unchanged; a threshold that would route every cell stops at the routing share of the deferred
+    rows (4096 + N / 128) instead of exhausting them."""
+    import paragram_b200.cuda as pc
+    from paragram_b200 import learned
+    from paragram_b200 import workloads as W
+
+    rng = np.random.default_rng(21)
+    train = [learned.collect(torch.from_numpy(W.surface_cloud(40_000, rng)).to(dev)) for _ in range(3)]
+    model = learned.train(train, epochs=4, batch=4096)
+    model.calibrate(train[0], quantile=0.97)
+    held = learned.collect(torch.from_numpy(W.surface_cloud(40_000, rng)).to(dev))
+    ok = held.weights > 0
+    pred = model.predicted_degree(held.features[ok]).cpu().numpy()
+    true = held.targets[ok, 1].double().cpu().numpy() * 16.0
+    assert np.corrcoef(pred, true)[0, 1] > 0.2  # the count output carries signal (weak on surfaces)
+
+    pts = W.surface_cloud(60_000, rng)
+    n = len(pts)
+    t = torch.from_numpy(pts).to(dev)
+    (a0, o0, s0), _ = pc.build_with_stats(t)
+    # deferred cells of the learned build without routing: the cells its first pass gives up on
+    model.set_route(0.0)
+    pc.build_with_stats(t, model=model.blob, profile=True)
+    base_deferred = pc.last_profile()["deferred_cells"]
+    route_cap = 4096 + n // 128
+    # a threshold that routes about 1% of the cells, and one that would route all of them
+    some = float(np.quantile(model.predicted_degree(learned.collect(t).features).cpu().numpy(), 0.99))
+    for thr, expect in ((some, "some"), (0.5, "capped")):
+        model.set_route(thr)
+        (a, o, s), st = pc.build_with_stats(t, model=model.blob, profile=True)
+        deferred = pc.last_profile()["deferred_cells"]
+        assert torch.equal(a, a0) and torch.equal(o, o0) and torch.equal(s, s0), thr
+        # deferred = routed cells + the unrouted ones the first pass gives up on
+        assert deferred > base_deferred, (thr, deferred, base_deferred)
+        routed = pc.last_profile()["routed_cells"]
+        assert 0 < routed <= deferred
+        if expect == "capped":
+            assert routed == route_cap
+            assert route_cap <= deferred <= route_cap + base_deferred, (deferred, route_cap)
+    oa, oo, os_ = oracle.diagram(pts)
+    assert np.array_equal(a.cpu().numpy(), oa) and np.array_equal(o.cpu().numpy(), oo)
