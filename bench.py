@@ -17,7 +17,9 @@ Workloads: clustered_voronoi_5m (default), clustered_voronoi_500k,
 uniform_voronoi_100k, uniform_power_1m, lattice_power_310 (29.8M-point jittered
 lattice, power: learned radius + batched CUDA-graph build, plain beside it;
 ``--plain`` for the single-cloud plain build), surface_batch_256 (256 surface
-clouds in one CUDA-graph batch).
+clouds in one CUDA-graph batch), moving_uniform_1m (iterations over 1M uniform
+points that move by 1% of their spacing between steps, each rebuilt with the
+previous step's diagram as initial guesses; the cold rebuild timed beside it).
 
 For N > 1 (torch.distributed.run, one process per GPU) every rank builds its
 own diagram of an equally sized, differently seeded point set (weak scaling;
@@ -58,6 +60,7 @@ WORKLOADS = {
     "lattice_power_310": dict(kind="lattice", n=310 ** 3, weighted=True),
     "surface_batch_256": dict(kind="surfaces", n=256, weighted=False),
     "surface_cloud_500k": dict(kind="surface", n=500_000, weighted=False),
+    "moving_uniform_1m": dict(kind="moving", n=1_000_000, weighted=False),
 }
 #: workloads built with the learned search radius (plain build timed beside them)
 LEARNED = {"clustered_voronoi_5m", "clustered_voronoi_500k"}
@@ -79,7 +82,17 @@ def make_points(spec: dict, seed: int):
         return W.surface_clouds(num_clouds=spec["n"], seed=seed), None
     if k == "surface":
         return W.surface_cloud(spec["n"], np.random.default_rng(seed)), None
+    if k == "moving":
+        return W.uniform(spec["n"], seed=seed), None
     raise ValueError(k)
+
+
+def moved_points(pts, seed: int):
+    """The moving workload's second point set: every point displaced by a Gaussian step of 1% of the
+    mean spacing of a unit-cube cloud of that size."""
+    rng = np.random.default_rng(7 + seed)
+    step_len = 0.01 * (1.0 / pts.shape[0]) ** (1.0 / 3.0)
+    return (pts + step_len * rng.standard_normal(pts.shape)).astype(np.float32)
 
 
 def train_model(dev, seed: int):
@@ -248,6 +261,15 @@ def run_reference_cuda(args, spec, world) -> bool:
             tot += len(c)
         calls = [(lambda t=t, **kw: pg_ref.voronoi(t, **kw)) for t in take]
         sample = f"the first {len(take)} of {len(pts)} clouds ({tot} points), one reference call per cloud"
+    elif spec["kind"] == "moving":
+        # the moved points, warm-started with the reference's own diagram of the previous positions
+        prev = pg_ref.voronoi(torch.from_numpy(pts).to(dev))
+        t = torch.from_numpy(moved_points(pts, 0)).to(dev)
+        g, go = prev[0].to(torch.int32).contiguous(), prev[1].to(torch.int32).contiguous()
+        calls = [(lambda **kw: pg_ref.voronoi(t, initial_guesses=g, initial_guesses_offsets=go, **kw))]
+        tot = len(pts)
+        sample = (f"the whole {tot}-point workload per step, moved points rebuilt with the reference's diagram of "
+                  "the previous positions as initial guesses")
     else:
         t = torch.from_numpy(pts).to(dev)
         tw = None if w is None else torch.from_numpy(w).to(dev)
@@ -481,6 +503,8 @@ def run_gpu(args, spec, rank, world, local):
         return run_batch_gpu(args, spec, rank, world, local, dev)
     if spec["kind"] == "lattice" and not args.plain:
         return run_lattice_gpu(args, spec, rank, world, local, dev)
+    if spec["kind"] == "moving":
+        return run_moving_gpu(args, spec, rank, world, local, dev)
     pts, w = make_points(spec, seed=rank)
     n = pts.shape[0]
     h_pts = torch.from_numpy(pts).pin_memory()
@@ -736,6 +760,103 @@ def run_lattice_gpu(args, spec, rank, world, local, dev):
             "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": n * 16, "d2h_bytes_per_step": d2h},
             "roofline": _roofline(flops, nbytes, cell_s, csum, "k_cells_fast (cell pass)", None),
             "cpu_baseline": _cpu_baseline(args, world, pts, w, n),
+            "clocks": csum,
+            "gpu_launches": int(prof["launches"]) * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_moving_gpu(args, spec, rank, world, local, dev):
+    """Warm start across iterations: the points move by 1% of their mean spacing between steps (a
+    fixed displacement field, applied forwards then backwards, so the steps alternate between two
+    point sets A and B), and each step rebuilds the diagram with the previous step's diagram as
+    initial guesses; the cold rebuild of the same points is timed beside it. Both give the same
+    diagram (checked here)."""
+    import torch
+
+    import paragram_b200 as pg
+    import paragram_b200.cuda as pc
+    from paragram_b200 import dist
+
+    pts, _ = make_points(spec, seed=rank)
+    n = pts.shape[0]
+    moved = moved_points(pts, rank)
+    h_sets = [torch.from_numpy(pts).pin_memory(), torch.from_numpy(moved).pin_memory()]
+    d_sets = [h.to(dev) for h in h_sets]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    diagrams = [pg.voronoi_diagram(d) for d in d_sets]  # each set's diagram, the guesses of the other
+    state = {"k": 0}
+
+    def step_warm():
+        k = state["k"] = 1 - state["k"]
+        prev = diagrams[1 - k]
+        return pc._run(d_sets[k], None, 8, False, prev.adjacency, prev.offsets, -1)
+
+    def step_cold():
+        return pc._run(d_sets[state["k"]], None, 8, False, None, None, -1)
+
+    host_out = _PinnedOut()
+
+    def step_e2e():
+        k = state["k"] = 1 - state["k"]
+        prev = diagrams[1 - k]
+        d = pg.voronoi_diagram(h_sets[k].to(dev, non_blocking=True), initial_guesses=prev.adjacency,
+                               initial_guesses_offsets=prev.offsets)
+        return host_out.copy("a", d.adjacency), host_out.copy("o", d.offsets), host_out.copy("s", d.status)
+
+    for _ in range(args.warmup):
+        step_warm()
+        step_cold()
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    times, cold_times, same = [], [], True
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            t, _, _, (a, o, s) = _timed(step_warm, 1, dev, flush)
+            times += t
+            t, _, _, (a0, o0, s0) = _timed(step_cold, 1, dev, flush)
+            cold_times += t
+            same = same and torch.equal(a, a0) and torch.equal(o, o0) and torch.equal(s, s0)
+    dist.barrier()
+    total_cells = dist.reduce_sum(float(n) * args.steps, dev)
+    value = total_cells / (dist.reduce_max(sum(times), dev) / 1e3) / 1e6
+    cold_value = total_cells / (dist.reduce_max(sum(cold_times), dev) / 1e3) / 1e6
+    for _ in range(max(1, args.warmup // 2)):
+        step_e2e()
+    e2e_times, _, _, (a, o, s) = _timed(step_e2e, args.steps, dev, flush)
+    e2e_value = total_cells / (dist.reduce_max(sum(e2e_times), dev) / 1e3) / 1e6
+    d2h = a.numel() * 4 + o.numel() * 4 + s.numel() * 4
+    k = 1 - state["k"]
+    prev = diagrams[1 - k]
+    _, cw = pc.build_with_stats(d_sets[k], initial_guesses=prev.adjacency, initial_guesses_offsets=prev.offsets,
+                                profile=True)
+    prof = pc.last_profile()
+    _, cc = pc.build_with_stats(d_sets[k])
+    if rank == 0:
+        off_np = diagrams[k].offsets.cpu().numpy()
+        flops, nbytes = algorithmic_work(off_np, False)
+        cell_s = (prof["cells_ms"] + prof["deferred_ms"]) / 1e3
+        csum = clocks.summary()
+        work = ("nodes", "leaves", "candidates", "clips")
+        line = {
+            "metric": "Mcells/s", "value": value, "unit": "Mcells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": statistics.mean(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "step_ms": [round(t, 2) for t in times],
+            "config": {"workload": args.workload, "n_points": n, "weighted": False,
+                       "motion": "1% of the mean spacing per step (Gaussian), alternating between two point sets",
+                       "warm_start": "the previous step's diagram as initial_guesses",
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"independent diagram per GPU x{world}",
+                       "cold": {"value": cold_value, "unit": "Mcells/s", "ms_per_step": statistics.mean(cold_times)},
+                       "warm_over_cold": value / cold_value, "identical_to_cold": bool(same),
+                       "work_per_cell_warm": {k_: round(cw[k_] / n, 3) for k_ in work},
+                       "work_per_cell_cold": {k_: round(cc[k_] / n, 3) for k_ in work},
+                       "phases_ms": {k_: round(prof[k_], 3) for k_ in ("lbvh_ms", "cells_ms", "deferred_ms",
+                                                                       "csr_ms")}},
+            "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": n * 12, "d2h_bytes_per_step": d2h},
+            "roofline": _roofline(flops, nbytes, cell_s, csum, "k_cells_fast (cell pass)", None),
+            "cpu_baseline": _cpu_baseline(args, world, pts, None, n),
             "clocks": csum,
             "gpu_launches": int(prof["launches"]) * args.steps,
         }

@@ -50,9 +50,12 @@ def load():
     return mod
 
 
-def voronoi(points, *, knn: int = 8, debug: bool = False, leaf_size: int = -1):
-    """The reference's build_voronoi_ultra on a CUDA (N, 3) float32 tensor."""
-    return load().build_voronoi_ultra(points.contiguous(), knn=knn, debug=debug, leaf_size=leaf_size)
+def voronoi(points, *, knn: int = 8, debug: bool = False, leaf_size: int = -1, initial_guesses=None,
+            initial_guesses_offsets=None):
+    """The reference's build_voronoi_ultra on a CUDA (N, 3) float32 tensor (initial guesses: int32
+    CUDA tensors, as its binding takes them, ext.cpp:21-29)."""
+    return load().build_voronoi_ultra(points.contiguous(), knn=knn, debug=debug, initial_guesses=initial_guesses,
+                                      initial_guesses_offsets=initial_guesses_offsets, leaf_size=leaf_size)
 
 
 def power(points, weights, *, knn: int = 8, debug: bool = False, leaf_size: int = -1):

@@ -5,6 +5,7 @@
 // pack -> BVH + kNN -> chunked cell kernel -> gather -> symmetrise -> cumsum
 // -> populate. Here: LBVH -> chunked cell launches -> deferred-cell pass ->
 // CSR count + scan (offsets) -> [host reads E] -> CSR fill.
+#include <atomic>
 #include <algorithm>
 #include <chrono>
 #include <cstdio>
@@ -106,11 +107,37 @@ size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
     return off;
 }
 
+// Total memory of the current device, queried once per device.
+static size_t device_total_memory()
+{
+    static std::atomic<size_t> total[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
+    {
+        cudaGetLastError();
+        return 0;
+    }
+    size_t t = total[dev].load();
+    if (t == 0)
+    {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, dev) == cudaSuccess)
+            t = prop.totalGlobalMem;
+        cudaGetLastError();
+        total[dev].store(t);
+    }
+    return t;
+}
+
 // Chunk plan of the cell pass. Mirrors plan_convex_cell_chunks (chunking.h:16-56):
 // PARAGRAM_NUM_CHUNKS forces a count; otherwise the per-cell scratch is compared
 // with PARAGRAM_MEM_FRAC (0.05 < f < 0.95, default 0.5) of the free device
 // memory. The clipper keeps its per-cell polyhedron in shared memory, so its
-// only per-cell global scratch is the directed row (kRowWidth ints).
+// only per-cell global scratch is the directed row (kRowWidth ints). The free
+// memory is queried only when the scratch exceeds that fraction of a quarter of
+// the device's total memory (never below 2^26 points on a B200): the query
+// takes the driver's lock, and a build that waited for it left the GPU idle
+// between its launches.
 static int plan_chunks(int64_t n, int requested)
 {
     if (requested > 0)
@@ -126,13 +153,16 @@ static int plan_chunks(int64_t n, int requested)
         if (f > 0.05 && f < 0.95)
             frac = f;
     }
+    size_t full = (size_t)n * kRowWidth * sizeof(int);
+    const size_t total = device_total_memory();
+    if (total > 0 && (double)full <= frac * (double)(total / 4))
+        return 1;
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess)
     {
         cudaGetLastError();
         return 1;
     }
-    size_t full = (size_t)n * kRowWidth * sizeof(int);
     size_t budget = (size_t)(frac * (double)free_b);
     if (budget > 0 && full > budget)
         return (int)((full + budget - 1) / budget);

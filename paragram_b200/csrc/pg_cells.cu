@@ -1866,18 +1866,35 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
     cudaMemsetAsync(ws.counters, 0, sizeof(int), st); // work counter
     int64_t cells = cl.cell_end - cl.cell_begin;
     // variants: register budget (2 or 3 blocks per SM), initial guesses, search radius per cell
-    // (a search radius is not used together with initial guesses)
     void (*kern)(CellArgs);
     if (cl.guesses)
-        kern = k_cells_fast<kMinBlocksLo, true, false>;
+        kern = cl.use_hint ? k_cells_fast<kMinBlocksLo, true, true> : k_cells_fast<kMinBlocksLo, true, false>;
     else if (cl.use_hint)
         kern = cl.min_blocks == 3 ? k_cells_fast<kMinBlocksHi, false, true> : k_cells_fast<kMinBlocksLo, false, true>;
     else
         kern = cl.min_blocks == 3 ? k_cells_fast<kMinBlocksHi, false, false> : k_cells_fast<kMinBlocksLo, false, false>;
+    // resident blocks per SM of this variant, queried once per (variant, device) and thread
+    struct Occ
+    {
+        void (*kern)(CellArgs);
+        int dev, blocks;
+    };
+    static thread_local Occ occ[16];
+    static thread_local int occ_n = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
     int blocks_per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerBlock * 32, 0);
-    if (blocks_per_sm < 1)
-        blocks_per_sm = 1;
+    for (int k = 0; k < occ_n; ++k)
+        if (occ[k].kern == kern && occ[k].dev == dev)
+            blocks_per_sm = occ[k].blocks;
+    if (blocks_per_sm == 0)
+    {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, kern, kWarpsPerBlock * 32, 0);
+        if (blocks_per_sm < 1)
+            blocks_per_sm = 1;
+        if (occ_n < 16)
+            occ[occ_n++] = Occ{kern, dev, blocks_per_sm};
+    }
     A.big_cap = cl.big_cap;
     A.route_cap = cl.route_cap;
     int64_t grid = std::min<int64_t>((int64_t)num_sms * blocks_per_sm, big_warps() / kWarpsPerBlock);

@@ -30,6 +30,7 @@
 // gradients contract over the samples: a block stages 64 samples' activations
 // and deltas transposed in shared memory and each warp owns a 16-row slice of
 // every weight gradient across all chunks of the batch.
+#include <atomic>
 #include <cuda_bf16.h>
 
 #include "../../include/paragram_b200.h"
@@ -827,11 +828,15 @@ int pg_mlp_grad(int64_t n, const float *features, const float *targets, const fl
         return PG_OK;
     cudaStream_t st = (cudaStream_t)stream;
     size_t smem = sizeof(GradSmem);
-    static bool attr = false;
-    if (!attr)
+    // the shared-memory opt-in is a per-device attribute of the kernel: set once per device
+    static std::atomic<unsigned long long> attr{0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (!(attr.load() & bit))
     {
         cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
+        attr.fetch_or(bit);
     }
     int64_t chunks = (n + kChunk - 1) / kChunk;
     int64_t grid = std::min<int64_t>(chunks, 148 * 4);

@@ -32,7 +32,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._api import Diagram, _validate_points, _validate_weights
+from ._api import Diagram, _validate_initial_guesses, _validate_points, _validate_weights
 
 NFEAT = 16
 NPARAM = 5378
@@ -262,23 +262,31 @@ def train(data: Sequence[Samples] | Samples, *, epochs: int = 4, batch: int = 81
     return model
 
 
-def _build(points, weights, model: Model):
+def _build(points, weights, model: Model, initial_guesses=None, initial_guesses_offsets=None):
     from . import cuda as pc
 
     w = None if weights is None else weights.reshape(-1, 1)
-    return pc._run(points, w, 8, False, None, None, -1, model=model.blob)
+    g, go = _validate_initial_guesses(initial_guesses, initial_guesses_offsets, points.shape[0], points.device)
+    return pc._run(points, w, 8, False, g, go, -1, model=model.blob)
 
 
-def voronoi_diagram(points: torch.Tensor, model: Model) -> Diagram:
-    """``paragram_b200.voronoi_diagram`` with the learned search radius (identical result)."""
+def voronoi_diagram(points: torch.Tensor, model: Model, *, initial_guesses: Optional[torch.Tensor] = None,
+                    initial_guesses_offsets: Optional[torch.Tensor] = None) -> Diagram:
+    """``paragram_b200.voronoi_diagram`` with the learned search radius (identical result).
+
+    ``initial_guesses`` / ``initial_guesses_offsets`` as in ``paragram_b200.voronoi_diagram`` (for
+    instance the previous diagram of slightly moved points): the cells are clipped by them first,
+    then searched with the learned radius."""
     points = _validate_points(points)
-    a, o, s = _build(points, None, model)
+    a, o, s = _build(points, None, model, initial_guesses, initial_guesses_offsets)
     return Diagram(adjacency=a, offsets=o, status=s)
 
 
-def power_diagram(points: torch.Tensor, weights: torch.Tensor, model: Model) -> Diagram:
+def power_diagram(points: torch.Tensor, weights: torch.Tensor, model: Model, *,
+                  initial_guesses: Optional[torch.Tensor] = None,
+                  initial_guesses_offsets: Optional[torch.Tensor] = None) -> Diagram:
     """``paragram_b200.power_diagram`` with the learned search radius (identical result)."""
     points = _validate_points(points)
     weights = _validate_weights(weights, points.shape[0], points.device)
-    a, o, s = _build(points, weights, model)
+    a, o, s = _build(points, weights, model, initial_guesses, initial_guesses_offsets)
     return Diagram(adjacency=a, offsets=o, status=s)

@@ -325,3 +325,35 @@ def test_search_radius_saves_candidates(dev, oracle):
     assert st2["hint_misses"] == 0
     assert st2["candidates"] < 0.8 * st["candidates"], (st2["candidates"], st["candidates"])
     assert st2["clips"] < st["clips"]
+
+
+def test_iterative_warm_start(dev, oracle):
+    """Points that move a little between iterations, each iteration rebuilt with the previous
+    iteration's diagram as initial guesses (plain, and with the learned search radius): every
+    rebuild equals the cold build of the same points and the oracle, and the warm start saves
+    traversal work (fewer BVH nodes and fewer clips per cell than the cold build)."""
+    import paragram_b200 as pg
+    import paragram_b200.cuda as pc
+    from paragram_b200 import learned
+    from paragram_b200 import workloads as W
+
+    n = 200_000
+    rng = np.random.default_rng(31)
+    x = W.uniform(n, seed=31)
+    step = 0.01 * (1.0 / n) ** (1.0 / 3.0)
+    model = learned.train([learned.collect(torch.from_numpy(W.uniform(n, seed=32)).to(dev))], epochs=2, batch=8192)
+    model.calibrate(learned.collect(torch.from_numpy(W.uniform(n, seed=33)).to(dev)), quantile=0.98)
+    prev = pg.voronoi_diagram(torch.from_numpy(x).to(dev))
+    for it in range(3):
+        x = (x + step * rng.standard_normal(x.shape)).astype(np.float32)
+        t = torch.from_numpy(x).to(dev)
+        (a0, o0, s0), cold = pc.build_with_stats(t)
+        (a1, o1, s1), warm = pc.build_with_stats(t, initial_guesses=prev.adjacency,
+                                                 initial_guesses_offsets=prev.offsets)
+        assert torch.equal(a1, a0) and torch.equal(o1, o0) and torch.equal(s1, s0), it
+        assert warm["nodes"] < cold["nodes"] and warm["clips"] < cold["clips"], (it, warm, cold)
+        d = learned.voronoi_diagram(t, model, initial_guesses=prev.adjacency, initial_guesses_offsets=prev.offsets)
+        assert torch.equal(d.adjacency, a0) and torch.equal(d.offsets, o0) and torch.equal(d.status, s0), it
+        if it == 0:
+            _assert_same((a1.cpu().numpy(), o1.cpu().numpy(), s1.cpu().numpy()), oracle.diagram(x), "warm start")
+        prev = pg.Diagram(adjacency=a1, offsets=o1, status=s1)
