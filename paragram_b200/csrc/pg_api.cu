@@ -300,7 +300,6 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     cl.weighted = weights != nullptr;
     cl.min_blocks = opt.blocks_per_sm == 3 ? 3 : 2; // register budget of the cell kernel
     cl.big_cap = big_cap(n);
-    cl.route_cap = route_cap(n);
     cl.fp32_only = opt.predicates == 1;
     cl.radius_out = opt.radius_out;
     cl.work_out = opt.work_out;
@@ -316,7 +315,7 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
         cudaMemcpyAsync(opt.order_out, ws.oid, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice, st);
     if (opt.model != nullptr)
     {
-        predict_launch(ws, n, num_clouds, (const pg_model *)opt.model, st);
+        predict_launch(ws, n, num_clouds, (const pg_model *)opt.model, status, route_cap(n), st);
         cl.use_hint = 1;
     }
     else if (opt.radius_hint != nullptr)

@@ -128,7 +128,6 @@ struct CellArgs
     int64_t begin, end;
     int big_pass;
     int64_t big_cap;
-    int64_t route_cap;
     char *slabs;
     char *huge_slabs;
     float *radius_out; // optional per-cell diagnostics (original ids)
@@ -1274,21 +1273,6 @@ __device__ __forceinline__ void process_cell(CellMem<CAP, STACK> &m, WarpState<C
     if (A.hint != nullptr)
     {
         float rq = A.hint[i];
-        if (rq < 0.0f)
-        {
-            // the model predicts more neighbours than the first pass's slots hold: deferred
-            // to the 128-slot tier before any traversal, while the routing share of the
-            // deferred rows lasts
-            int r = 0;
-            if (lane == 0)
-                r = atomicAdd(&A.counters[7], 1);
-            if (__shfl_sync(kFull, r, 0) < A.route_cap)
-            {
-                ws.flags |= kFlagDefer;
-                return;
-            }
-            rq = -rq;
-        }
         if (rq > 0.0f && rq < 1e30f)
             cap = rq;
     }
@@ -1663,6 +1647,9 @@ __device__ __forceinline__ void cells_body(CellMem<CAP, STACK> &m, const CellArg
         if (t >= count)
             break;
         int i = A.big_pass ? A.big_list[t] : (int)(A.begin + t);
+        // a cell the learned model routed to the 128-slot tier (listed by the prediction)
+        if (HINT && A.hint != nullptr && A.hint[i] < 0.0f)
+            continue;
         PG_T0(tcell);
         process_cell<CAP, STACK, GUESS, HINT>(m, ws, i, A, lane);
         write_diagnostics(m, ws, A, lane);
@@ -1842,7 +1829,6 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.end = cl.cell_end;
     A.big_pass = 0;
     A.big_cap = 0;
-    A.route_cap = 0;
     A.slabs = (char *)ws.big_slabs;
     A.huge_slabs = (char *)ws.huge_slabs;
     A.radius_out = cl.radius_out;
@@ -1896,7 +1882,6 @@ void cells_launch(const Workspace &ws, const CellLaunch &cl, int *status, int nu
             occ[occ_n++] = Occ{kern, dev, blocks_per_sm};
     }
     A.big_cap = cl.big_cap;
-    A.route_cap = cl.route_cap;
     int64_t grid = std::min<int64_t>((int64_t)num_sms * blocks_per_sm, big_warps() / kWarpsPerBlock);
     int64_t need = (cells + kWarpsPerBlock - 1) / kWarpsPerBlock;
     if (grid > need)

@@ -35,7 +35,6 @@ struct CellLaunch
     int weighted;
     int min_blocks; // register-budget variant of the cell kernel (2 or 3 blocks per SM)
     int64_t big_cap; // deferred-row slots
-    int64_t route_cap; // of which at most this many for cells the model routes past the first pass
     float *radius_out; // per original id: certified radius of the final cell, or nullptr
     int *work_out;     // per original id: nodes, leaves, candidates, peak queue; or nullptr
     float *geometry_out; // per original id: centroid x, y, z and volume of the cell; or nullptr
@@ -51,7 +50,11 @@ void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, in
 
 // pg_mlp.cu
 void features_launch(const Workspace &ws, int64_t n, int num_clouds, float *out, cudaStream_t st);
-void predict_launch(const Workspace &ws, int64_t n, int num_clouds, const ::pg_model *model, cudaStream_t st);
+// The learned radius of every sorted slot into ws.hint; with the model's route_degree set, the
+// slots predicted at or above it (at most route_cap) are listed for the 128-slot tier, their
+// rows marked deferred and their hint negated (the first pass skips them).
+void predict_launch(const Workspace &ws, int64_t n, int num_clouds, const ::pg_model *model, int *status,
+                    int64_t route_cap, cudaStream_t st);
 int set_last_error(int code, const std::string &msg);
 
 // pg_csr.cu

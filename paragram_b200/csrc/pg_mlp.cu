@@ -372,12 +372,37 @@ __device__ __forceinline__ void store_normalized(const MlpSmem &S, const float (
         row[k] = __float2bfloat16_rn((f[k] - S.mean[k]) * S.scale[k]);
 }
 
+// Where the prediction lists the cells it routes past the first pass.
+struct Route
+{
+    int *counters;   // [1]: deferred cells, [7]: routing requests
+    int *big_list;   // deferred sorted slots
+    int *deg;        // directed degree by original index
+    int *status;     // status by original index
+    const int *oid;  // sorted slot -> original index
+    int64_t cap;     // at most this many routed cells
+};
+
+// A routed cell: listed for the 128-slot tier with a placeholder row (an empty row whose
+// plane_overflow status the deferred pass replaces), while the routing share lasts.
+__device__ __forceinline__ bool route_cell(const Route &rt, int64_t i)
+{
+    if ((int64_t)atomicAdd(&rt.counters[7], 1) >= rt.cap)
+        return false;
+    int d = atomicAdd(&rt.counters[1], 1);
+    rt.big_list[d] = (int)i;
+    int o = rt.oid[i];
+    rt.deg[o] = 0;
+    rt.status[o] = kPlaneOverflow;
+    return true;
+}
+
 // Search radius of each sorted slot from its features (the cell pass's cap).
 // Block = 8 warps, a warp predicts 32 consecutive slots.
 __global__ void __launch_bounds__(256) k_mlp_predict(int64_t n, const float4 *__restrict__ pts,
                                                      const int *__restrict__ bounds, const int *__restrict__ cloud_off,
                                                      int num_clouds, const pg_model *__restrict__ model,
-                                                     float *__restrict__ hint)
+                                                     float *__restrict__ hint, Route rt)
 {
     __shared__ MlpSmem S;
     __shared__ __align__(16) __nv_bfloat16 xr[8][32 * kS16];
@@ -424,11 +449,12 @@ __global__ void __launch_bounds__(256) k_mlp_predict(int64_t n, const float4 *__
                     {
                         float ly = F.y[2 * h] / S.tscale[0] + S.tmean[0] + S.margin + lref_r;
                         float rad = expf(ly);
-                        // a predicted neighbour count at or above route_degree: negative radius,
-                        // the cell pass sends the cell to its 128-slot tier directly
+                        // a predicted neighbour count at or above route_degree: the cell is listed
+                        // for the 128-slot tier and its radius negated (the first pass skips it)
                         float deg = (F.y[2 * h + 1] / S.tscale[1] + S.tmean[1]) * 16.0f;
-                        bool route = S.route > 0.0f && deg >= S.route;
-                        hint[ir] = (lref_r == lref_r && rad < 1e30f) ? (route ? -rad : rad) : 0.0f;
+                        bool ok_r = lref_r == lref_r && rad < 1e30f;
+                        bool routed = ok_r && S.route > 0.0f && deg >= S.route && route_cell(rt, ir);
+                        hint[ir] = ok_r ? (routed ? -rad : rad) : 0.0f;
                     }
                 }
             }
@@ -786,13 +812,15 @@ void features_launch(const Workspace &ws, int64_t n, int num_clouds, float *out,
                                                              out);
 }
 
-void predict_launch(const Workspace &ws, int64_t n, int num_clouds, const pg_model *model, cudaStream_t st)
+void predict_launch(const Workspace &ws, int64_t n, int num_clouds, const pg_model *model, int *status,
+                    int64_t route_cap, cudaStream_t st)
 {
     int64_t warps = (n + 31) / 32;
     int64_t grid = std::min<int64_t>((warps + 7) / 8, 148 * 8);
+    Route rt{ws.counters, ws.big_list, ws.deg, status, ws.oid, route_cap};
     ++g_launches;
     k_mlp_predict<<<(unsigned)std::max<int64_t>(grid, 1), 256, 0, st>>>(n, ws.pts, ws.bounds, ws.cloud_off,
-                                                                        num_clouds, model, ws.hint);
+                                                                        num_clouds, model, ws.hint, rt);
 }
 
 } // namespace pg
