@@ -124,6 +124,7 @@ class ClockSampler:
         self.gpu = gpu_index
         self.samples = []
         self._stop = threading.Event()
+        self._first = threading.Event()
         self._thr = None
 
     def _run(self):
@@ -132,6 +133,7 @@ class ClockSampler:
                                   "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
                                  stderr=subprocess.DEVNULL, text=True)
         except OSError:
+            self._first.set()
             return
         try:
             while not self._stop.is_set():
@@ -139,13 +141,19 @@ class ClockSampler:
                 if not line:
                     break
                 self.samples.append([x.strip() for x in line.split(",")])
+                self._first.set()
         finally:
+            self._first.set()
             p.kill()
             p.wait()
 
     def __enter__(self):
         self._thr = threading.Thread(target=self._run, daemon=True)
         self._thr.start()
+        # the sampler's start-up (driver initialisation) must not overlap the first timed step:
+        # wait for its first sample and a moment more
+        self._first.wait(timeout=10)
+        time.sleep(0.3)
         return self
 
     def __exit__(self, *a):
