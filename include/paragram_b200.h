@@ -178,7 +178,29 @@ int pg_emit_adjacency(int64_t num_points, const void *workspace, const int32_t *
  * (the reference only prints timings, voronoi_ultra.cu:196-219). */
 int pg_stats(const void *workspace, int64_t num_points, uint64_t *out, int32_t count, void *stream);
 
-/* Where the BVH lives inside a workspace that pg_build (num_clouds = 1) or pg_build_batch
+/* ---- One diagram over several GPUs (no reference counterpart: the reference builds on one
+ * device). Every rank holds all points (an all-gather of their shards), builds the LBVH and the
+ * cells of its own range of sorted slots, and exchanges its rows:
+ *   pg_build_range   the LBVH of all points and the cells of sorted slots [cell_begin, cell_end)
+ *                    (the curve order of the LBVH: equal ranges are balanced and compact); status
+ *                    [num_points] receives those cells' statuses. Synchronises the stream.
+ *   pg_range_pack    the range's rows as one int32 pack: count, the cells' point indices [count],
+ *                    statuses [count], row starts [count + 1], then the neighbour indices. With
+ *                    pack == NULL only *words_needed is set (synchronises the stream).
+ *   pg_range_unpack  another rank's pack (count = its cell_end - cell_begin) into this workspace.
+ *   pg_range_finish  the symmetric CSR offsets of the assembled rows and the edge count
+ *                    (synchronises); pg_emit_adjacency then fills the adjacency as after pg_build.
+ * Every rank that unpacks all other ranks' packs holds the same Diagram as a single pg_build. */
+int pg_build_range(int64_t num_points, const float *points, const float *weights, const pg_options *options,
+                   void *workspace, size_t workspace_bytes, int64_t cell_begin, int64_t cell_end, int32_t *status,
+                   void *stream);
+int pg_range_pack(int64_t num_points, const void *workspace, const int32_t *status, int64_t cell_begin,
+                  int64_t cell_end, int32_t *pack, int64_t pack_words, int64_t *words_needed, void *stream);
+int pg_range_unpack(int64_t num_points, void *workspace, int32_t *status, const int32_t *pack, int64_t count,
+                    int64_t pack_words, void *stream);
+int pg_range_finish(int64_t num_points, void *workspace, int32_t *offsets, int64_t *num_edges, void *stream);
+
+/* Where the BVH lives inside a workspace/* Where the BVH lives inside a workspace that pg_build (num_clouds = 1) or pg_build_batch
  * filled: out[k] = byte offset from the workspace's start of
  *   [0] the sorted points (float4 x, y, z, w per sorted slot, N of them),
  *   [1] sorted slot -> original point index (int32 [N]),
@@ -192,6 +214,17 @@ int pg_stats(const void *workspace, int64_t num_points, uint64_t *out, int32_t c
  * For inspection and tests (the layout depends on num_points and num_clouds only).
  * No reference counterpart (the reference's BVH is cuBQL's, pwr_bvh.cu:42-339). */
 int pg_workspace_tree(int64_t num_points, int32_t num_clouds, int64_t *out, int32_t count);
+
+/* The k nearest other points of every point (1 <= k <= 32): neighbours [num_points * k] receives,
+ * per point in input order, the original indices of its k nearest points by unweighted FP32
+ * Euclidean distance (ties by index; the point itself excluded, copies at its position included),
+ * -1 where the cloud has fewer points. Builds the LBVH in workspace (pg_workspace_size bytes,
+ * 256-byte aligned) and synchronises the stream. Replaces the reference's kNN query
+ * (pwr_bvh.cu:159-215), which warm-starts its cells (voronoi_ultra.cu:205-227); here the cell pass
+ * does not need it (its traversal starts at the point's own leaf), and a caller that wants the
+ * reference's warm start passes the result to pg_build as initial guesses. */
+int pg_knn(int64_t num_points, const float *points, int32_t k, void *workspace, size_t workspace_bytes,
+           int32_t *neighbours, void *stream);
 
 /* Profile of the last pg_build + pg_emit_adjacency on this thread:
  * out[0] kernel launches, out[1] LBVH ms, out[2] cell pass ms, out[3] deferred-cell

@@ -9,6 +9,7 @@ fallback -- calling the API without the built library raises ImportError.
 from ._api import Diagram, power_diagram, voronoi_diagram
 from .batch import build_batch
 from .geometry import cell_geometry, cell_vertices, face_areas
+from .neighbours import knn
 
 __all__ = [
     "Diagram",
@@ -16,6 +17,7 @@ __all__ = [
     "cell_geometry",
     "cell_vertices",
     "face_areas",
+    "knn",
     "power_diagram",
     "voronoi_diagram",
 ]

@@ -80,13 +80,24 @@ def power_diagram(
     initial_guesses: Optional[torch.Tensor] = None,
     initial_guesses_offsets: Optional[torch.Tensor] = None,
     leaf_size: int = -1,
+    knn_warm_start: bool = False,
 ) -> Diagram:
-    """Weighted 3D power (Laguerre) diagram. Reference: paragram/_api.py:65-94."""
+    """Weighted 3D power (Laguerre) diagram. Reference: paragram/_api.py:65-94.
+
+    ``knn`` is accepted like the reference's and, by default, not needed: the cell traversal starts
+    at the point's own BVH leaf. ``knn_warm_start=True`` clips every cell by its ``knn`` nearest
+    points first, as the reference does (the same diagram, more work)."""
     points = _validate_points(points)
     weights = _validate_weights(weights, points.shape[0], points.device)
     initial_guesses, initial_guesses_offsets = _validate_initial_guesses(
         initial_guesses, initial_guesses_offsets, points.shape[0], points.device
     )
+    if knn_warm_start and initial_guesses is None and knn > 0:
+        # the reference's warm start: clip every cell by its knn nearest points first (results
+        # do not change; given initial guesses take precedence, as in voronoi_ultra.cu:155-162)
+        from .neighbours import knn_guesses
+
+        initial_guesses, initial_guesses_offsets = knn_guesses(points, knn)
     from .cuda import build_laguerre_voronoi_ultra
 
     adjacency, offsets, status = build_laguerre_voronoi_ultra(
@@ -109,12 +120,20 @@ def voronoi_diagram(
     initial_guesses: Optional[torch.Tensor] = None,
     initial_guesses_offsets: Optional[torch.Tensor] = None,
     leaf_size: int = -1,
+    knn_warm_start: bool = False,
 ) -> Diagram:
-    """Unweighted 3D Voronoi diagram. Reference: paragram/_api.py:97-123."""
+    """Unweighted 3D Voronoi diagram. Reference: paragram/_api.py:97-123 (``knn`` and
+    ``knn_warm_start`` as in ``power_diagram``)."""
     points = _validate_points(points)
     initial_guesses, initial_guesses_offsets = _validate_initial_guesses(
         initial_guesses, initial_guesses_offsets, points.shape[0], points.device
     )
+    if knn_warm_start and initial_guesses is None and knn > 0:
+        # the reference's warm start: clip every cell by its knn nearest points first (results
+        # do not change; given initial guesses take precedence, as in voronoi_ultra.cu:155-162)
+        from .neighbours import knn_guesses
+
+        initial_guesses, initial_guesses_offsets = knn_guesses(points, knn)
     from .cuda import build_voronoi_ultra
 
     adjacency, offsets, status = build_voronoi_ultra(

@@ -43,7 +43,8 @@ class PgOptions(ctypes.Structure):
 EXPORTED = ["pg_version", "pg_last_error", "pg_workspace_size", "pg_build", "pg_emit_adjacency", "pg_stats",
             "pg_last_profile", "pg_degrees_to_offsets_noalloc", "pg_batch_workspace_size", "pg_build_batch",
             "pg_batch_check", "pg_mlp_num_params", "pg_mlp_model_bytes", "pg_mlp_forward", "pg_mlp_grad",
-            "pg_mlp_adam", "pg_mlp_pack", "pg_face_areas", "pg_workspace_tree"]
+            "pg_mlp_adam", "pg_mlp_pack", "pg_face_areas", "pg_workspace_tree", "pg_knn", "pg_build_range",
+            "pg_range_pack", "pg_range_unpack", "pg_range_finish"]
 
 
 def load() -> ctypes.CDLL:
@@ -70,6 +71,16 @@ def load() -> ctypes.CDLL:
         lib.pg_emit_adjacency.restype = ctypes.c_int
         lib.pg_stats.argtypes = [vp, i64, ctypes.POINTER(ctypes.c_uint64), i32, vp]
         lib.pg_stats.restype = ctypes.c_int
+        lib.pg_build_range.argtypes = [i64, vp, vp, ctypes.POINTER(PgOptions), vp, sz, i64, i64, vp, vp]
+        lib.pg_build_range.restype = ctypes.c_int
+        lib.pg_range_pack.argtypes = [i64, vp, vp, i64, i64, vp, i64, ctypes.POINTER(i64), vp]
+        lib.pg_range_pack.restype = ctypes.c_int
+        lib.pg_range_unpack.argtypes = [i64, vp, vp, vp, i64, i64, vp]
+        lib.pg_range_unpack.restype = ctypes.c_int
+        lib.pg_range_finish.argtypes = [i64, vp, vp, ctypes.POINTER(i64), vp]
+        lib.pg_range_finish.restype = ctypes.c_int
+        lib.pg_knn.argtypes = [i64, vp, i32, vp, sz, vp, vp]
+        lib.pg_knn.restype = ctypes.c_int
         lib.pg_workspace_tree.argtypes = [i64, i32, ctypes.POINTER(i64), i32]
         lib.pg_workspace_tree.restype = ctypes.c_int
         lib.pg_last_profile.argtypes = [ctypes.POINTER(ctypes.c_double), i32]

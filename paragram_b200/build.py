@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD_DIR = os.path.join(HERE, "_build")
 LIB_PATH = os.path.join(HERE, "libparagram_b200.so")
 SOURCES = ["pg_api.cu", "pg_lbvh.cu", "pg_cells.cu", "pg_csr.cu", "pg_scan.cu", "pg_noalloc.cu", "pg_mlp.cu",
-           "pg_faces.cu"]
+           "pg_faces.cu", "pg_knn.cu"]
 #: The instrumented variant (per-phase SM cycle counters in the cell kernel, -DPG_PHASE_CYCLES): a
 #: separate library for profiling only; ``PARAGRAM_B200_LIB`` selects it at load time.
 PHASE_BUILD_DIR = os.path.join(HERE, "_build_phase")

@@ -194,6 +194,96 @@ __global__ void k_hint_gather(int64_t n, const int *oid, const float *radius, fl
         hint[i] = fmaxf(radius[oid[i]], 0.0f);
 }
 
+// ---- One diagram over several GPUs: every rank builds the LBVH of all points and the cells of
+// its own range of sorted slots, packs its rows, receives the others' packs and assembles the CSR.
+// A pack (int32 words): count, the cells' original indices [count], statuses [count], row starts
+// [count + 1] (exclusive scan of the degrees), then the rows' neighbour indices.
+
+// The row of original point u: the fast-pass row, or (deferred cells) a deferred-row slot.
+__device__ __forceinline__ const int *shard_row(const int *rows, const int *big_rows, const int *deg, int u, int &d)
+{
+    int dv = deg[u];
+    if (dv & (int)kBigFlag)
+    {
+        d = dv & ~(int)kBigFlag;
+        return big_rows + (size_t)rows[(size_t)u * kRowWidth] * kBigRowWidth;
+    }
+    d = dv;
+    return rows + (size_t)u * kRowWidth;
+}
+
+__global__ void k_pack_degrees(int64_t begin, int64_t count, const int *oid, const int *deg, uint32_t *sizes)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < count)
+        sizes[t] = (uint32_t)(deg[oid[begin + t]] & ~(int)kBigFlag);
+    else if (t == count)
+        sizes[t] = 0u;
+}
+
+__global__ void k_pack_rows(int64_t begin, int64_t count, const int *oid, const int *rows, const int *big_rows,
+                            const int *deg, const int *status, const uint32_t *start, int *out)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t > count)
+        return;
+    int *ids = out + 1, *sts = ids + count;
+    int *st = sts + count, *nb = st + count + 1;
+    st[t] = (int)start[t];
+    if (t == count)
+    {
+        out[0] = (int)count;
+        return;
+    }
+    int u = oid[begin + t], d = 0;
+    const int *r = shard_row(rows, big_rows, deg, u, d);
+    ids[t] = u;
+    sts[t] = status[u];
+    int *o = nb + start[t];
+    for (int j = 0; j < d; ++j)
+        o[j] = r[j];
+}
+
+// Rows of another rank's cells into this workspace: fast-pass rows where they fit, else a
+// deferred-row slot after the ones in use. Flags: 4 = no deferred-row slot left, 5 = malformed pack.
+__global__ void k_unpack_rows(int64_t n, int64_t count, int64_t words, const int *pack, int *rows, int *big_rows,
+                              int *deg, int *status, int *counters, int64_t big_capacity)
+{
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count)
+        return;
+    const int *ids = pack + 1, *sts = ids + count, *st = sts + count, *nb = st + count + 1;
+    const int64_t nb_words = words - (2 + 3 * count);
+    int u = ids[t], s0 = st[t], s1 = st[t + 1];
+    int d = s1 - s0;
+    if (u < 0 || u >= n || s0 < 0 || d < 0 || d > kBigRowWidth || (int64_t)s1 > nb_words)
+    {
+        atomicExch(&counters[2], 5);
+        return;
+    }
+    int *row;
+    if (d <= kRowWidth)
+    {
+        row = rows + (size_t)u * kRowWidth;
+        deg[u] = d;
+    }
+    else
+    {
+        int slot = atomicAdd(&counters[1], 1);
+        if ((int64_t)slot >= big_capacity)
+        {
+            atomicExch(&counters[2], 4);
+            return;
+        }
+        row = big_rows + (size_t)slot * kBigRowWidth;
+        rows[(size_t)u * kRowWidth] = slot;
+        deg[u] = d | (int)kBigFlag;
+    }
+    for (int j = 0; j < d; ++j)
+        row[j] = nb[s0 + j];
+    status[u] = sts[t];
+}
+
 static int check_counters(const int *host, int64_t n)
 {
     if (host[2] == 1)
@@ -201,6 +291,10 @@ static int check_counters(const int *host, int64_t n)
                                      "polytope topology)");
     if (host[2] == 2)
         return fail(PG_ERR_INTERNAL, "a cloud's points do not form one BVH subtree");
+    if (host[2] == 4)
+        return fail(PG_ERR_INTERNAL, "received rows exceed the deferred-row capacity");
+    if (host[2] == 5)
+        return fail(PG_ERR_INVALID, "malformed row pack");
     if (host[1] > big_cap(n))
         return fail(PG_ERR_INTERNAL, "too many cells exceeded 64 vertices (" + std::to_string(host[1]) +
                                          " > capacity " + std::to_string(big_cap(n)) + ")");
@@ -213,8 +307,12 @@ static int check_counters(const int *host, int64_t n)
 static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, const float *points,
                       const float *weights, const int32_t *guesses, const int32_t *guess_off,
                       const pg_options *options, void *workspace, size_t workspace_bytes, int32_t *offsets,
-                      int32_t *status, int64_t *num_edges, void *stream)
+                      int32_t *status, int64_t *num_edges, void *stream, int64_t range_begin = 0,
+                      int64_t range_end = -1)
 {
+    // range_end >= 0: only the cells of sorted slots [range_begin, range_end), no CSR (a shard of a
+    // diagram built on several GPUs; pg_build_range)
+    const bool ranged = range_end >= 0;
     g_last_error.clear();
     cudaStream_t st = (cudaStream_t)stream;
     pg_options opt{};
@@ -225,8 +323,10 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     const bool sync = num_edges != nullptr;
     if (n < 0 || n >= kMaxPoints)
         return fail(PG_ERR_INVALID, "num_points must be in [0, 2^26)");
-    if (!offsets)
+    if (!offsets && !ranged)
         return fail(PG_ERR_INVALID, "offsets must not be NULL");
+    if (ranged && (range_begin < 0 || range_begin > range_end || range_end > n))
+        return fail(PG_ERR_INVALID, "the cell range must lie within [0, num_points]");
     if ((guesses == nullptr) != (guess_off == nullptr))
         return fail(PG_ERR_INVALID, "initial_guesses and initial_guesses_offsets must be provided together");
     if (n > 0 && (!points || !status || !workspace))
@@ -253,7 +353,8 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     cudaGetLastError();
     if (n == 0)
     {
-        cudaMemsetAsync(offsets, 0, sizeof(int32_t), st);
+        if (offsets)
+            cudaMemsetAsync(offsets, 0, sizeof(int32_t), st);
         if (!sync)
             return PG_OK;
         *num_edges = 0;
@@ -326,11 +427,12 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     }
     int chunks = sync ? plan_chunks(n, opt.num_chunks) : std::max(opt.num_chunks, 1);
     int sms = device_sms();
-    int64_t per = (n + chunks - 1) / chunks;
+    const int64_t rb = ranged ? range_begin : 0, re = ranged ? range_end : n;
+    int64_t per = (re - rb + chunks - 1) / chunks;
     for (int c = 0; c < chunks; ++c)
     {
-        cl.cell_begin = (int64_t)c * per;
-        cl.cell_end = std::min<int64_t>(n, cl.cell_begin + per);
+        cl.cell_begin = rb + (int64_t)c * per;
+        cl.cell_end = std::min<int64_t>(re, cl.cell_begin + per);
         if (cl.cell_begin >= cl.cell_end)
             break;
         cells_launch(ws, cl, status, sms, st);
@@ -342,7 +444,8 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     cells_big_launch(ws, cl, status, big_cap(n), st);
     if (timing)
         cudaEventRecord(ev[2], st);
-    csr_count(ws, n, offsets, st);
+    if (!ranged)
+        csr_count(ws, n, offsets, st);
     g_profile[0] = (double)g_launches;
     g_profile[6] = (double)chunks;
     if (!sync)
@@ -354,7 +457,8 @@ static int build_impl(int64_t n, int num_clouds, const int32_t *cloud_offsets, c
     int64_t edges = 0;
     {
         uint32_t e32 = 0;
-        cudaMemcpyAsync(&e32, offsets + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (!ranged)
+            cudaMemcpyAsync(&e32, offsets + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         cudaMemcpyAsync(host, ws.counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, st);
         cudaError_t e = cudaStreamSynchronize(st);
         if (e != cudaSuccess)
@@ -473,6 +577,97 @@ int pg_batch_check(const void *workspace, int64_t total_points, int32_t num_clou
     if (e != cudaSuccess)
         return fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
     return check_counters(host, total_points);
+}
+
+int pg_build_range(int64_t n, const float *points, const float *weights, const pg_options *options, void *workspace,
+                   size_t workspace_bytes, int64_t cell_begin, int64_t cell_end, int32_t *status, void *stream)
+{
+    int64_t unused = 0;
+    return pg::build_impl(n, 1, nullptr, points, weights, nullptr, nullptr, options, workspace, workspace_bytes,
+                          nullptr, status, &unused, stream, cell_begin, cell_end);
+}
+
+int pg_range_pack(int64_t n, const void *workspace, const int32_t *status, int64_t cell_begin, int64_t cell_end,
+                  int32_t *pack, int64_t pack_words, int64_t *words_needed, void *stream)
+{
+    using namespace pg;
+    g_last_error.clear();
+    if (n < 0 || n >= kMaxPoints || cell_begin < 0 || cell_begin > cell_end || cell_end > n)
+        return fail(PG_ERR_INVALID, "need 0 <= cell_begin <= cell_end <= num_points < 2^26");
+    if (!workspace || !status || !words_needed)
+        return fail(PG_ERR_INVALID, "workspace, status and words_needed must not be NULL");
+    Workspace ws;
+    workspace_layout(n, 1, (char *)workspace, &ws);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t count = cell_end - cell_begin;
+    const unsigned g = (unsigned)((count + 1 + 255) / 256);
+    ++g_launches;
+    k_pack_degrees<<<g, 256, 0, st>>>(cell_begin, count, ws.oid, ws.deg, ws.sizes);
+    exclusive_scan(ws.sizes, ws.sizes, count + 1, ws.scan_tmp, st);
+    uint32_t total = 0;
+    cudaMemcpyAsync(&total, ws.sizes + count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    const int64_t need = 2 + 3 * count + (int64_t)total;
+    *words_needed = need;
+    if (!pack)
+        return PG_OK;
+    if (pack_words < need)
+        return fail(PG_ERR_INVALID, "pack too small: need " + std::to_string(need) + " words");
+    ++g_launches;
+    k_pack_rows<<<g, 256, 0, st>>>(cell_begin, count, ws.oid, ws.rows, ws.big_rows, ws.deg, status, ws.sizes, pack);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? PG_OK : fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+}
+
+int pg_range_unpack(int64_t n, void *workspace, int32_t *status, const int32_t *pack, int64_t count,
+                    int64_t pack_words, void *stream)
+{
+    using namespace pg;
+    g_last_error.clear();
+    if (n < 0 || n >= kMaxPoints || count < 0 || count > n)
+        return fail(PG_ERR_INVALID, "need 0 <= count <= num_points < 2^26");
+    if (!workspace || !status || !pack)
+        return fail(PG_ERR_INVALID, "workspace, status and pack must not be NULL");
+    if (pack_words < 2 + 3 * count)
+        return fail(PG_ERR_INVALID, "pack shorter than its index");
+    if (count == 0)
+        return PG_OK;
+    Workspace ws;
+    workspace_layout(n, 1, (char *)workspace, &ws);
+    cudaStream_t st = (cudaStream_t)stream;
+    ++g_launches;
+    k_unpack_rows<<<(unsigned)((count + 255) / 256), 256, 0, st>>>(n, count, pack_words, pack, ws.rows, ws.big_rows,
+                                                                   ws.deg, status, ws.counters, big_cap(n));
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? PG_OK : fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+}
+
+int pg_range_finish(int64_t n, void *workspace, int32_t *offsets, int64_t *num_edges, void *stream)
+{
+    using namespace pg;
+    g_last_error.clear();
+    if (n < 0 || n >= kMaxPoints)
+        return fail(PG_ERR_INVALID, "num_points must be in [0, 2^26)");
+    if (!workspace || !offsets || !num_edges)
+        return fail(PG_ERR_INVALID, "workspace, offsets and num_edges must not be NULL");
+    Workspace ws;
+    workspace_layout(n, 1, (char *)workspace, &ws);
+    cudaStream_t st = (cudaStream_t)stream;
+    csr_count(ws, n, offsets, st);
+    int host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t e32 = 0;
+    cudaMemcpyAsync(&e32, offsets + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(host, ws.counters, 8 * sizeof(int), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess)
+        return fail(PG_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    int rc = check_counters(host, n);
+    if (rc != PG_OK)
+        return rc;
+    *num_edges = e32;
+    return PG_OK;
 }
 
 int pg_emit_adjacency(int64_t n, const void *workspace, const int32_t *offsets, int32_t *adjacency, void *stream)
