@@ -513,6 +513,8 @@ def run_gpu(args, spec, rank, world, local):
         return run_lattice_gpu(args, spec, rank, world, local, dev)
     if spec["kind"] == "moving":
         return run_moving_gpu(args, spec, rank, world, local, dev)
+    if args.sharded:
+        return run_sharded_gpu(args, spec, rank, world, local, dev)
     pts, w = make_points(spec, seed=rank)
     n = pts.shape[0]
     h_pts = torch.from_numpy(pts).pin_memory()
@@ -774,6 +776,72 @@ def run_lattice_gpu(args, spec, rank, world, local, dev):
         print(json.dumps(line), flush=True)
 
 
+def run_sharded_gpu(args, spec, rank, world, local, dev):
+    """One diagram over all ranks (strong scaling, ``--sharded``): the workload's one point set
+    (seed 0 on every rank) split into contiguous shards, rank r passing the r-th; every step is
+    ``paragram_b200.sharded.voronoi_diagram`` / ``power_diagram`` (point all-gather, the rank's
+    range of cells, row all-gather, CSR assembly), which returns the full Diagram on every rank.
+    The plain build (no learned radius)."""
+    import torch
+
+    import paragram_b200.cuda as pc
+    from paragram_b200 import dist, sharded
+
+    pts, w = make_points(spec, seed=0)
+    n = pts.shape[0]
+    b, e = n * rank // world, n * (rank + 1) // world
+    h_pts = torch.from_numpy(np.ascontiguousarray(pts[b:e])).pin_memory()
+    h_w = None if w is None else torch.from_numpy(np.ascontiguousarray(w[b:e])).pin_memory()
+    d_pts = h_pts.to(dev)
+    d_w = None if h_w is None else h_w.to(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def build(p, wt):
+        return sharded.voronoi_diagram(p) if wt is None else sharded.power_diagram(p, wt)
+
+    host_out = _PinnedOut()
+
+    def step_e2e():
+        d = build(h_pts.to(dev, non_blocking=True), None if h_w is None else h_w.to(dev, non_blocking=True))
+        return host_out.copy("a", d.adjacency), host_out.copy("o", d.offsets), host_out.copy("s", d.status)
+
+    for _ in range(args.warmup):
+        build(d_pts, d_w)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    with ClockSampler(local) as clocks:
+        times, _, launches, d = _timed(lambda: build(d_pts, d_w), args.steps, dev, flush)
+    dist.barrier()
+    total_ms = dist.reduce_max(sum(times), dev)
+    value = float(n) * args.steps / (total_ms / 1e3) / 1e6
+    step_e2e()
+    e2e_times, _, _, (a, o, s) = _timed(step_e2e, args.steps, dev, flush)
+    e2e_value = float(n) * args.steps / (dist.reduce_max(sum(e2e_times), dev) / 1e3) / 1e6
+    d2h = a.numel() * 4 + o.numel() * 4 + s.numel() * 4
+    if rank == 0:
+        off_np = d.offsets.cpu().numpy()
+        flops, nbytes = algorithmic_work(off_np, spec["weighted"])
+        csum = clocks.summary()
+        line = {
+            "metric": "Mcells/s", "value": value, "unit": "Mcells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "step_ms": [round(t, 2) for t in times],
+            "config": {"workload": args.workload, "n_points": n, "weighted": spec["weighted"],
+                       "parallelism": f"one diagram sharded over {world} GPU(s): point all-gather, a range of "
+                                      "the curve order per rank, row all-gather, CSR on every rank",
+                       "l2": "flushed between steps (256 MiB write)"},
+            "e2e": {"value": e2e_value, "unit": "Mcells/s", "h2d_bytes_per_step": h_pts.numel() * 4 +
+                    (0 if h_w is None else h_w.numel() * 4), "d2h_bytes_per_step": d2h},
+            "roofline": _roofline(flops / world, nbytes / world, total_ms / args.steps / 1e3, csum,
+                                  "whole sharded step (this rank's share of the cells)", None),
+            "cpu_baseline": None,
+            "clocks": csum,
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_moving_gpu(args, spec, rank, world, local, dev):
     """Warm start across iterations: the points move by 1% of their mean spacing between steps (a
     fixed displacement field, applied forwards then backwards, so the steps alternate between two
@@ -957,6 +1025,8 @@ def main():
                     help="with --impl reference: time the CPU restatement even where the reference's CUDA "
                          "extension is built")
     ap.add_argument("--plain", action="store_true", help="time the plain build only (no learned radius)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="strong scaling: one diagram of the workload built by all ranks together")
     ap.add_argument("--fp32-only-too", action="store_true",
                     help="also time the build with FP32-only side tests (no FP64 / exact escalation)")
     args = ap.parse_args()

@@ -119,6 +119,8 @@ def exchange(local: torch.Tensor, group=None) -> list[torch.Tensor]:
     order (lengths first, then the tensors padded to the longest)."""
     import torch.distributed as dist
 
+    if not (dist.is_available() and dist.is_initialized()):
+        return [local]  # one process: nothing to exchange
     world = dist.get_world_size(group)
     size = torch.tensor([local.numel()], dtype=torch.int64, device=local.device)
     sizes = [torch.zeros_like(size) for _ in range(world)]
@@ -135,7 +137,10 @@ def exchange(local: torch.Tensor, group=None) -> list[torch.Tensor]:
 def _diagram(points_local: torch.Tensor, weights_local: Optional[torch.Tensor], group, leaf_size: int) -> Diagram:
     import torch.distributed as dist
 
-    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    if dist.is_available() and dist.is_initialized():
+        rank, world = dist.get_rank(group), dist.get_world_size(group)
+    else:
+        rank, world = 0, 1
     points = torch.cat(exchange(points_local.reshape(-1), group)).reshape(-1, 3).contiguous()
     weights = None
     if weights_local is not None:

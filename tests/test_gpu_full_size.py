@@ -115,3 +115,46 @@ def test_lattice_310_power(dev, oracle):
     exp = _oracle(oracle, pts, w)
     bad = _diff_cells(got, exp)
     assert bad.size == 0, f"{bad.size} cells differ, first {bad[:5].tolist()}"
+
+
+def test_max_size_uniform(dev, oracle):
+    """The largest input the LBVH's leaf references allow, N = 2^26 - 1 uniform points (1.04G
+    directed entries): the build completes with every status 0 or 2, every row sorted and the CSR
+    symmetric (all entries, checked on the device), and the first 10,000 cells equal the oracle's
+    exact rows (the exact Voronoi diagram of points in general position has no empty cell and its
+    directed rows are already symmetric)."""
+    import paragram_b200 as pg
+    from paragram_b200 import workloads as W
+
+    n = (1 << 26) - 1
+    pts = W.uniform(n, seed=81)
+    d = pg.voronoi_diagram(torch.from_numpy(pts).to(dev))
+    adj, off, st = d.adjacency, d.offsets.long(), d.status
+    e = adj.numel()
+    assert int(off[-1]) == e and e > 14 * n
+    assert bool(((st == 0) | (st == 2)).all())
+    deg = off[1:] - off[:-1]
+    rows = torch.repeat_interleave(torch.arange(n, device=dev), deg)
+    # sorted rows: a row's entries increase; (row, column) keys are then globally sorted
+    keys = rows * n + adj.long()
+    del rows
+    assert bool((keys[1:] > keys[:-1]).all())
+    # symmetric: every (u, v) has its (v, u)
+    cols = adj.long()
+    rkeys = cols * n + torch.repeat_interleave(torch.arange(n, device=dev), deg)
+    del cols
+    pos = torch.searchsorted(keys, rkeys).clamp_max(e - 1)
+    assert bool((keys[pos] == rkeys).all())
+    del keys, rkeys, pos
+    m = 10_000
+    t0 = time.perf_counter()
+    c = oracle.cells(pts, None, begin=0, end=m)
+    print(f"oracle: {m} of {n} cells (kd-tree over all points) in {time.perf_counter() - t0:.1f} s")
+    got_off = off[: m + 1].cpu().numpy()
+    got = adj[: int(got_off[-1])].cpu().numpy()
+    exp_off = c.row_offsets.astype(np.int64)
+    rid = np.repeat(np.arange(m), np.diff(exp_off))
+    exp = c.rows.astype(np.int64)[np.lexsort((c.rows, rid))]
+    assert np.array_equal(got_off, exp_off)
+    assert np.array_equal(got.astype(np.int64), exp)
+    assert np.array_equal(st[:m].cpu().numpy(), c.status)

@@ -66,3 +66,15 @@ def test_range_calls_reject_bad_arguments(dev):
     st = torch.empty(100, dtype=torch.int32, device=dev)
     assert lib.pg_range_pack(100, ws.data_ptr(), st.data_ptr(), 20, 10, None, 0, ctypes.byref(need), None) == -1
     assert lib.pg_range_unpack(100, ws.data_ptr(), st.data_ptr(), ws.data_ptr(), 10, 5, None) == -1
+
+
+def test_sharded_api_single_process(dev):
+    """Without a process group the sharded calls build the whole range on this GPU."""
+    import paragram_b200 as pg
+    from paragram_b200 import sharded
+    from paragram_b200 import workloads as W
+
+    pts, w = W.power_uniform(30_000, seed=76)
+    t, tw = torch.from_numpy(pts).to(dev), torch.from_numpy(w).to(dev)
+    assert _same(sharded.power_diagram(t, tw), pg.power_diagram(t, tw))
+    assert _same(sharded.voronoi_diagram(t), pg.voronoi_diagram(t))
