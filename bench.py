@@ -24,7 +24,9 @@ previous step's diagram as initial guesses; the cold rebuild timed beside it).
 For N > 1 (torch.distributed.run, one process per GPU) every rank builds its
 own diagram of an equally sized, differently seeded point set (weak scaling;
 cells shard without any data exchange) and the step time is the max over
-ranks. ``--impl reference`` times the reference's own CUDA extension
+ranks. ``--sharded`` times strong scaling instead: one diagram of the workload
+built by all ranks together (point all-gather, a range of cells per rank, row
+all-gather, the CSR on every rank). ``--impl reference`` times the reference's own CUDA extension
 (``oracle/_ref``: its unmodified sources compiled with a project-written
 stand-in for its absent cuBQL dependency) on the same workload, counting its
 construction phase (cells + CSR) by its own timers; without that build or a
