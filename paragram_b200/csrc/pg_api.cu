@@ -88,7 +88,6 @@ size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws)
     w.big_list2 = (int *)take(4 * (size_t)big_cap((int64_t)N));
     w.big_slot2 = (int *)take(4 * (size_t)big_cap((int64_t)N));
     w.big_rows = (int *)take(4 * (size_t)big_cap((int64_t)N) * kBigRowWidth);
-    w.big_slabs = take(big_slab_bytes());
     w.huge_slabs = take(huge_slab_bytes());
     w.cnt = (int *)take(4 * N);
     w.miss = (int *)take(4 * N);

@@ -33,7 +33,7 @@
 //
 // A cell that needs more than 64 vertex / plane slots is deferred to a second
 // launch with 128 slots in shared memory, and one that outgrows those to a
-// third with 256 slots in global memory (then 512); its status is then
+// third with 256 slots, also in shared memory (then 512 in a global slab); its status is then
 // vertex_overflow (2) if the final cell has more than 64 vertices (the
 // reference MAX_VERTS) and plane_overflow (1) only if even 512 slots overflow.
 //
@@ -128,7 +128,6 @@ struct CellArgs
     int64_t begin, end;
     int big_pass;
     int64_t big_cap;
-    char *slabs;
     char *huge_slabs;
     float *radius_out; // optional per-cell diagnostics (original ids)
     int4 *work_out;
@@ -1698,12 +1697,12 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, MINB) k_cells_fast(CellAr
 
 
 // Rebuild cell i with 256 vertex / plane slots and a 1024-entry queue in this
-// warp's global slab: a cell that outgrew the 128 slots of the middle tier. A
-// cell that outgrows the 256 slots too is rebuilt once more by huge_cell.
-template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, int i, int lane, int slot)
+// warp's share of the block's shared memory: a cell that outgrew the 128 slots
+// of the middle tier. A cell that outgrows the 256 slots too is rebuilt once
+// more by huge_cell.
+template <bool GUESS>
+__device__ __forceinline__ void big_cell(CellMem<kCapBig, kStackBig> &m, const CellArgs &A, int i, int lane, int slot)
 {
-    size_t gw = ((size_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    auto &m = *reinterpret_cast<CellMem<kCapBig, kStackBig> *>(A.slabs + gw * sizeof(CellMem<kCapBig, kStackBig>));
     WarpState<kCapBig> ws;
     if (lane < kNumStats)
         m.cnt[lane] = 0;
@@ -1725,7 +1724,7 @@ template <bool GUESS> __device__ __noinline__ void big_cell(const CellArgs &A, i
 
 // The middle tier's loop: the cells the first pass deferred (list index t =
 // their deferred-row slot), with 128 slots; a cell that outgrows them is listed
-// again for the global-memory tier. A separate body from the first pass's, whose
+// again for the 256-slot tier. A separate body from the first pass's, whose
 // code (one inlined copy of traversal and clip) is kept as it is.
 template <bool GUESS> __device__ __forceinline__ void mid_body(CellMem<kCapMid, kStackMid> &m, const CellArgs &A, int lane)
 {
@@ -1769,9 +1768,13 @@ template <bool GUESS> __device__ __forceinline__ void mid_body(CellMem<kCapMid, 
     flush_stats(m, A, lane);
 }
 
-// Global-memory tier: the cells that outgrew the middle tier, one per warp at a time.
-template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_cells_big(CellArgs A)
+// Third tier: the cells that outgrew the middle tier, one per warp at a time, each
+// warp's 256-slot state in shared memory (kBigWarps warps per block; the 512-slot
+// rebuilds keep theirs in global slabs).
+template <bool GUESS> __global__ void __launch_bounds__(kBigWarps * 32, 2) k_cells_big(CellArgs A)
 {
+    extern __shared__ __align__(16) unsigned char big_smem[];
+    auto *m = reinterpret_cast<CellMem<kCapBig, kStackBig> *>(big_smem) + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     const int64_t count = min((int64_t)A.counters[5], A.big_cap);
     for (;;)
@@ -1782,7 +1785,7 @@ template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32) k_c
         t = __shfl_sync(kFull, t, 0);
         if (t >= count)
             break;
-        big_cell<GUESS>(A, A.big_list2[t], lane, A.big_slot2[t]);
+        big_cell<GUESS>(*m, A, A.big_list2[t], lane, A.big_slot2[t]);
     }
 }
 
@@ -1797,9 +1800,8 @@ template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) 
     mid_body<GUESS>(*m, A, lane);
 }
 
-int big_warps() { return 148 * kMaxWarpsPerSM; } // one slab per resident warp
+int big_warps() { return 148 * kMaxWarpsPerSM; } // upper bound of resident cell warps
 size_t huge_slab_bytes() { return sizeof(CellMem<kCapHuge, kStackHuge>) * (size_t)kHugeSlabs; }
-size_t big_slab_bytes() { return sizeof(CellMem<kCapBig, kStackBig>) * (size_t)big_warps(); }
 
 static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
 {
@@ -1829,7 +1831,6 @@ static CellArgs make_args(const Workspace &ws, const CellLaunch &cl)
     A.end = cl.cell_end;
     A.big_pass = 0;
     A.big_cap = 0;
-    A.slabs = (char *)ws.big_slabs;
     A.huge_slabs = (char *)ws.huge_slabs;
     A.radius_out = cl.radius_out;
     A.work_out = reinterpret_cast<int4 *>(cl.work_out);
@@ -1914,13 +1915,17 @@ void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, in
     }
     ++g_launches;
     mid<<<(unsigned)(148 * 2), kWarpsPerBlock * 32, mid_smem, st>>>(A);
-    // one global slab per warp of this grid
-    unsigned grid = (unsigned)(big_warps() / kWarpsPerBlock);
+    // 2 blocks of kBigWarps warps per SM, 256-slot state in shared memory
+    const size_t big_smem = sizeof(CellMem<kCapBig, kStackBig>) * kBigWarps;
+    void (*bigk)(CellArgs) = cl.guesses ? k_cells_big<true> : k_cells_big<false>;
+    static std::atomic<unsigned long long> big_ready[2];
+    if (!(big_ready[cl.guesses ? 1 : 0].load() & bit))
+    {
+        cudaFuncSetAttribute(bigk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)big_smem);
+        big_ready[cl.guesses ? 1 : 0].fetch_or(bit);
+    }
     ++g_launches;
-    if (cl.guesses)
-        k_cells_big<true><<<grid, kWarpsPerBlock * 32, 0, st>>>(A);
-    else
-        k_cells_big<false><<<grid, kWarpsPerBlock * 32, 0, st>>>(A);
+    bigk<<<(unsigned)(148 * 2), kBigWarps * 32, big_smem, st>>>(A);
 }
 
 } // namespace pg

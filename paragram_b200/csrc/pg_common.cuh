@@ -36,7 +36,8 @@ constexpr int kBigRowWidth = kCapBig; // row slots of a deferred cell
 #define PG_WARPS_PER_BLOCK 8
 #endif
 constexpr int kWarpsPerBlock = PG_WARPS_PER_BLOCK; // cell kernel block, one cell per warp at a time
-constexpr int kMaxWarpsPerSM = 32;  // resident cell warps per SM the global slabs are sized for
+constexpr int kMaxWarpsPerSM = 32;  // upper bound of resident cell warps per SM (grid cap of the first pass)
+constexpr int kBigWarps = 4;        // warps per block of the 256-slot tier (state in shared memory)
 constexpr int kMaxLeaf = 32;        // leaf size limit (one candidate per lane)
 constexpr int kDefaultLeaf = 16;
 constexpr int kWindow = 16;         // optional warm start: sorted neighbours i-16 .. i+16
@@ -143,7 +144,6 @@ struct Workspace
     int *big_list2;       // [big_cap] sorted slots that outgrew the middle tier too
     int *big_slot2;       // [big_cap] their deferred-row slots
     int *big_rows;        // [big_cap * kBigRowWidth]
-    void *big_slabs;      // per-warp state of the large-capacity pass
     void *huge_slabs;     // [kHugeSlabs] state of cells that outgrew the large capacity
     // CSR
     int *cnt;             // [N] kept directed entries per row
@@ -154,8 +154,7 @@ struct Workspace
     size_t bytes;
 };
 
-int big_warps();   // number of warps of the large-capacity pass
-size_t big_slab_bytes();
+int big_warps();   // upper bound of resident cell warps on the device
 size_t huge_slab_bytes();
 size_t workspace_layout(int64_t n, int num_clouds, char *base, Workspace *ws);
 
