@@ -1792,7 +1792,7 @@ template <bool GUESS> __global__ void __launch_bounds__(kBigWarps * 32, 2) k_cel
 // Middle tier: the cells that outgrew 64 slots, with 128 slots and a 512-entry
 // queue in shared memory (its own launch, so its larger shared-memory carve-out
 // does not shrink the first pass's L1).
-template <bool GUESS> __global__ void __launch_bounds__(kWarpsPerBlock * 32, 2) k_cells_mid(CellArgs A)
+template <bool GUESS> __global__ void __launch_bounds__(kMidWarps * 32, kMidBlocksPerSM) k_cells_mid(CellArgs A)
 {
     extern __shared__ __align__(16) unsigned char mid_smem[];
     int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1901,7 +1901,7 @@ void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, in
     CellArgs A = make_args(ws, cl);
     A.status = status;
     A.big_cap = big_cap;
-    const size_t mid_smem = sizeof(CellMem<kCapMid, kStackMid>) * kWarpsPerBlock;
+    const size_t mid_smem = sizeof(CellMem<kCapMid, kStackMid>) * kMidWarps;
     void (*mid)(CellArgs) = cl.guesses ? k_cells_mid<true> : k_cells_mid<false>;
     // the shared-memory opt-in is a per-device attribute of the kernel: set once per device
     static std::atomic<unsigned long long> mid_ready[2];
@@ -1914,7 +1914,7 @@ void cells_big_launch(const Workspace &ws, const CellLaunch &cl, int *status, in
         mid_ready[cl.guesses ? 1 : 0].fetch_or(bit);
     }
     ++g_launches;
-    mid<<<(unsigned)(148 * 2), kWarpsPerBlock * 32, mid_smem, st>>>(A);
+    mid<<<(unsigned)(148 * kMidBlocksPerSM), kMidWarps * 32, mid_smem, st>>>(A);
     // 2 blocks of kBigWarps warps per SM, 256-slot state in shared memory
     const size_t big_smem = sizeof(CellMem<kCapBig, kStackBig>) * kBigWarps;
     void (*bigk)(CellArgs) = cl.guesses ? k_cells_big<true> : k_cells_big<false>;

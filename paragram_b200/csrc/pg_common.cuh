@@ -38,6 +38,8 @@ constexpr int kBigRowWidth = kCapBig; // row slots of a deferred cell
 constexpr int kWarpsPerBlock = PG_WARPS_PER_BLOCK; // cell kernel block, one cell per warp at a time
 constexpr int kMaxWarpsPerSM = 32;  // upper bound of resident cell warps per SM (grid cap of the first pass)
 constexpr int kBigWarps = 4;        // warps per block of the 256-slot tier (state in shared memory)
+constexpr int kMidWarps = 4;        // warps per block of the 128-slot tier (13 KB of shared memory each)
+constexpr int kMidBlocksPerSM = 3;  // its resident blocks per SM (up to 170 registers per thread)
 constexpr int kMaxLeaf = 32;        // leaf size limit (one candidate per lane)
 constexpr int kDefaultLeaf = 16;
 constexpr int kWindow = 16;         // optional warm start: sorted neighbours i-16 .. i+16
